@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the wave-propagation step on B200.
+
+Default workload (N = 1): the plain large case -- 4096^2 grid, FP64, minmod-limited second-order
+HLL wave propagation, 16 seeded Gaussian bumps (seed 0), CFL 0.9, 500 accepted steps.  A
+"step" is one attempted time step (xi sweep, eta sweep, time control, ghost fill).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl reference]
+
+Multi-GPU (torchrun, one process per GPU): independent replicas of the workload, one per GPU
+(the step has no exchange between grids); `value` is the aggregate over ranks and the time is
+the max over ranks.  `--impl reference` times the CPU restatement of the reference (LAPACK
+dgeev per interface, OpenMP over the host cores) on a bounded row band of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s FP64 vs mixed @L1(h)≤1e-5; batched solve p50/p99 latency"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL_SWEEP = 48          # read 3 x 8 B + write 3 x 8 B of state per cell per sweep
+BYTES_PER_CELL_UPDATE = 96         # two sweeps
+
+
+def workload(m: int):
+    from paraclaws_b200 import control as ctl
+    c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=1.0e9)
+    return c
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            pass
+    return {}
+
+
+def hbm_peak():
+    pk = measured_peaks()
+    if "hbm_gbs" in pk:
+        return float(pk["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, workload_name: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "ncu_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and parts[1] == workload_name:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in Path(self.path).read_text().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+# ------------------------------------------------------------------------------------------
+# CPU baseline: the oracle (restatement of the reference) on the host cores
+# ------------------------------------------------------------------------------------------
+def cpu_band_run(m: int, rows: int, steps: int, eigen_mode: int, threads: int):
+    """Time `steps` attempted steps of the oracle on rows 1..rows of the m x m workload."""
+    import dataclasses
+
+    import numpy as np
+
+    from oracle import oracle
+    from paraclaws_b200 import ic
+    oracle.build()
+    oracle.set_threads(threads)
+    c = workload(m)
+    d_eta = (c.eta_max - c.eta_min) / m
+    band = dataclasses.replace(c, m_eta=rows, eta_max=c.eta_min + rows * d_eta)
+    full_x, _ = ic.cell_centres(m, m)
+    q = ic.gaussian_bumps(m, m, seed=0)[: rows + 4].copy()
+    o = oracle.Oracle(band, eigen_mode=eigen_mode)
+    o.set_state(q)
+    o.update_rank_boundaries()
+    t0 = time.perf_counter()
+    log = o.run(max_attempts=steps)
+    dt = time.perf_counter() - t0
+    acc = int(log.accepted)
+    o.close()
+    return acc * m * rows, dt
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(m: int) -> dict:
+    thr = cpu_threads()
+    # calibrate the band so the faithful (LAPACK dgeev) sample is ~15 s of work
+    cells, dt = cpu_band_run(m, 16, 1, eigen_mode=1, threads=thr)
+    per_cell = dt / max(cells, 1)
+    rows = int(max(16, min(m, 15.0 / max(per_cell * m, 1e-12))))
+    cells, dt = cpu_band_run(m, rows, 1, eigen_mode=1, threads=thr)
+    faithful = cells / dt
+    cells_c, dt_c = cpu_band_run(m, rows, 2, eigen_mode=0, threads=thr)
+    return {"value": faithful, "unit": UNIT, "cores": thr, "kind": "port",
+            "sample": f"1 step of a {m} x {rows} row band of the {m}^2 workload, reference call structure with "
+                      f"LAPACK dgeev/BLAS dgemv per interface (scipy OpenBLAS), OpenMP {thr} threads",
+            "closed_form_value": cells_c / dt_c,
+            "closed_form_sample": f"2 steps of the same band, closed-form eigenvalues"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    m = args.grid
+    thr = cpu_threads()
+    budget = 150.0  # seconds for the whole warmup + steps run
+    cells, dt = cpu_band_run(m, 16, 1, eigen_mode=1, threads=thr)
+    per_cell = dt / max(cells, 1)
+    rows = int(max(4, min(m, budget / (args.steps + args.warmup) / max(per_cell * m, 1e-12))))
+    cpu_band_run(m, rows, args.warmup, eigen_mode=1, threads=thr)
+    cells, dt = cpu_band_run(m, rows, args.steps, eigen_mode=1, threads=thr)
+    value = cells / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / max(args.steps, 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": "port",
+                         "sample": f"each step: one attempted step of a {m} x {rows} row band of the {m}^2 "
+                                   f"workload; CPU restatement of the reference (Fortran not buildable here) "
+                                   f"with LAPACK dgeev/BLAS dgemv per interface, OpenMP {thr} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def aggregate_over_ranks(dist, ms: float, accepted: int, device) -> tuple:
+    """Replicas: the job time is the slowest rank's, the work is the sum over ranks."""
+    import torch
+    if dist is None:
+        return ms, accepted
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    a = torch.tensor([float(accepted)], dtype=torch.float64, device=device)
+    dist.all_reduce(a, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(a.item())
+
+
+def config_dict(args) -> dict:
+    return {"workload": f"plain-large: {args.grid}^2 dam-break grid, 16 seeded Gaussian bumps (seed 0), "
+                        f"minmod-limited second-order HLL, CFL 0.9, {args.steps} accepted steps",
+            "grid": args.grid, "precision": args.precision, "limiter": "minmod", "bc": "zero-gradient",
+            "l2": "inputs larger than L2 (state buffer %.0f MB > 126 MB)" % (3 * 8 * (args.grid + 4) ** 2 / 1e6),
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200 import ic
+    from paraclaws_b200.solver import Solver, run_host_loop
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    m = args.grid
+    prec = ctl.PRECISION_MIXED if args.precision == "mixed" else ctl.PRECISION_FP64
+    c = workload(m)
+    cu = ctl.CustomSettings(max_accepted_steps=args.steps, precision_mode=prec)
+    q = ic.gaussian_bumps(m, m, seed=0)
+    s = Solver(c, cu, device=local)
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
+
+    def restart():
+        s.upload(q)
+        s.update_rank_boundaries()
+        s.reset_time_control()
+
+    # warmup: W attempted steps, then restart from the initial condition
+    restart()
+    s.advance(max_attempts=args.warmup)
+    restart()
+    s.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = s.stats().launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        st = s.advance(max_attempts=args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = st.launches - l0
+    accepted = st.accepted
+    ms_max, acc_total = aggregate_over_ranks(dist, ms, accepted, torch.device("cuda", local))
+    value = acc_total * m * m / (ms_max * 1e-3)
+
+    # per-kernel durations (CUDA events on the context's stream) for the roofline, on a fresh
+    # start of the same workload so every kernel does its full work
+    restart()
+    s.advance(max_attempts=args.warmup)
+    kms = s.profile_kernels(reps=10)
+    if prec == ctl.PRECISION_FP64:
+        names = ["xsweep_fp64", "ysweep_fp64", "timectl", "ghost"]
+        sweep_ms = {names[0]: kms[0], names[1]: kms[1]}
+        bytes_per_launch = BYTES_PER_CELL_SWEEP * m * m
+    else:
+        names = ["sweep_mixed", "timectl", "ghost"]
+        sweep_ms = {names[0]: kms[0]}
+        bytes_per_launch = BYTES_PER_CELL_UPDATE * m * m
+    dom = max(sweep_ms, key=sweep_ms.get)
+    peak, peak_kind = hbm_peak()
+    achieved = bytes_per_launch / (sweep_ms[dom] * 1e-3) / 1e9
+    wl_name = f"grid{m}"
+    traffic = ncu_traffic(dom, wl_name)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "traffic": traffic, "algorithmic_bytes_per_launch": bytes_per_launch,
+                "kernel_ms": {names[k]: kms[k] for k in range(len(kms))},
+                "step_bytes_effective_GBps": value * BYTES_PER_CELL_UPDATE / 1e9}
+
+    # e2e: the reference-facing C-ABI, driven from the host like main.f90, with host buffers
+    e2e = None
+    if rank == 0 or True:
+        import ctypes as C
+        nbytes = q.nbytes
+        hptr = C.c_void_p()
+        s.L.pcl_host_alloc(C.byref(hptr), nbytes)
+        hq = np.frombuffer((C.c_char * nbytes).from_address(hptr.value), dtype=np.float64).reshape(q.shape)
+        hq[...] = q
+        hout = np.empty_like(q)
+        s.reset_time_control()
+        io0 = s.io_bytes()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.upload(hq)
+        s.update_rank_boundaries()
+        lg = run_host_loop(s, max_attempts=args.steps)
+        s.download(hout)
+        e1.record(stream)
+        e1.synchronize()
+        ems = e0.elapsed_time(e1)
+        n_att = max(len(lg.dt), 1)
+        acc_e = int((lg.ierr > 0).sum())
+        io1 = s.io_bytes()
+        h2d = io1["h2d"] - io0["h2d"]
+        d2h = io1["d2h"] - io0["d2h"]
+        e2e = {"value": acc_e * m * m / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d / n_att, "d2h_bytes_per_step": d2h / n_att,
+               "path": "host-driven main loop through the C ABI (pcl_solve_dimensional_split, "
+                       "pcl_update_rank_boundaries, pcl_update_time, ...), IC uploaded from pinned host "
+                       "memory and the final state downloaded inside the timed region",
+               "steps": n_att}
+        s.L.pcl_host_free(hptr)
+        if dist is not None:
+            ems_max, acc_all = aggregate_over_ranks(dist, ems, acc_e, torch.device("cuda", local))
+            e2e["value"] = acc_all * m * m / (ems_max * 1e-3)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == ctl.PRECISION_FP64 else "f32+f64",
+        "data": "synthetic", "config": config_dict(args), "roofline": roofline, "e2e": e2e,
+        "gpu_launches": launches, "clocks": clocks.summary(), "accepted_steps": accepted,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(m)
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--grid", type=int, default=4096)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

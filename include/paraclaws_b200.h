@@ -1,0 +1,168 @@
+/*
+ * paraclaws_b200.h -- C ABI of the B200-native wave-propagation finite-volume step.
+ *
+ * The drop-in boundary for paraCLAWs' hot path: the Fortran host keeps read_solver_control,
+ * the user equation module and the time loop of main.f90, and binds these entry points with
+ * iso_c_binding (bind(C) interfaces: see INTEGRATION.md).  Plain C types only; all arrays
+ * are caller-owned host buffers; every call returns an int status (PCL_OK = 0, errors < 0).
+ *
+ * Threading: one host thread per context; each context owns one CUDA stream and its device
+ * memory; there is no global state besides the CUDA device.
+ *
+ * State layout at the boundary is the reference's: vars(3, -1:m_xi+2, -1:m_eta+2) column-major
+ * (domain/SMOD_domain_allocation.f90:94), (h, hu, hv) fastest.  Inside the context the state is
+ * held as SoA planes in device memory; the transpose happens only in upload/download.
+ */
+#ifndef PARACLAWS_B200_H
+#define PARACLAWS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PCL_OK 0
+#define PCL_ERR_NAN (-1)        /* NaN in a flux Jacobian (examples/2D_dam_break/cartesian/SMOD_jakobian.f90:55-70) */
+#define PCL_ERR_NEG_DEPTH (-2)  /* h < 0: complex eigenvalues (utility/SMOD_eigenvalue_problem.f90:72-83) */
+#define PCL_ERR_TIMEOUT (-3)    /* a bounded device wait gave up */
+#define PCL_ERR_OOM (-4)        /* device or pinned-host allocation failed */
+#define PCL_ERR_BADARG (-5)     /* invalid settings or arguments */
+#define PCL_ERR_CUDA (-6)       /* CUDA runtime error */
+#define PCL_ERR_FATAL_DT (-7)   /* end_program in updateTime (time_control/MOD_time_control.f90:213-231) */
+#define PCL_ERR_IO (-8)         /* control.in / custom.in unreadable */
+#define PCL_ERR_FULL (-9)       /* batch: no free slot or over the memory budget */
+
+/* precision forms (custom.in) */
+#define PCL_PREC_FP64 0   /* bit-compatible FP64 path (the drop-in) */
+#define PCL_PREC_MIXED 1  /* FP32 flux/limiter arithmetic, FP64 state, FP64 dt and sums */
+
+/* boundary-condition codes (user_subroutines/SMOD_boundary_conditions.f90:13) */
+#define PCL_BC_WALL 1          /* BC_USER slot: reflective wall in this build */
+#define PCL_BC_ZERO_GRADIENT 2
+#define PCL_BC_CONST_GRADIENT 3
+
+/* Everything read_solver_control reads from control.in (utility/MOD_IO.f90:61-94), in that
+   order, plus the settings this build reads from custom.in (the reference leaves custom.in
+   unread: custom_settings.py:16-22). */
+typedef struct pcl_solver_control {
+  int num_equations, num_dimensions, num_ghost, num_aux, num_waves;
+  int number_of_snapshots;
+  int adaptive_timestepping;
+  int higher_order_flux_correction;
+  int use_limiter;
+  int limiter_method;
+  int m_xi, m_eta;
+  int bc_xi_lower, bc_xi_upper, bc_eta_lower, bc_eta_upper;
+  int precision_mode;           /* custom.in */
+  int initial_condition;        /* custom.in: 0 file, 1 circular dam */
+  double t_start, t_final, dt_initial, cfl_limit, dt_min, dt_max;
+  double dt_max_growth_ratio, dt_min_shrink_ratio;
+  double xi_min, xi_max, eta_min, eta_max;
+  double grav;                  /* custom.in; the reference sets it in SMOD_setup.f90:21 */
+  double dam_radius, dam_h_in, dam_h_out, dam_x0, dam_y0;  /* custom.in */
+  long long max_accepted_steps; /* custom.in: 0 = run to t_final only */
+} pcl_solver_control;
+
+typedef struct pcl_ctx pcl_ctx;
+
+/* Per-run counters of a context. */
+typedef struct pcl_run_stats {
+  long long attempts, accepted, rejected;
+  long long launches;           /* kernels this context has launched so far */
+  double time, dt, dt_previous, cfl;
+  int snapshot_index, done, status, last_ierr;
+} pcl_run_stats;
+
+/* One attempted step as main.f90:265-271 reports it. */
+typedef struct pcl_step_record {
+  double dt, cfl, time, dt_next;
+  int ierr, snapshot_index;
+} pcl_step_record;
+
+/* ---- configuration ---- */
+
+/* Fill *out with the reference defaults (control_settings.py:21-105; grav = real(9.81)). */
+void pcl_default_control(pcl_solver_control* out);
+
+/* Parse control.in (28 list-directed records, utility/MOD_IO.f90:55-94) and, if custom_in is
+   not NULL and exists, this build's custom.in.  Replaces read_solver_control's reads. */
+int pcl_read_solver_control(const char* control_in, const char* custom_in, pcl_solver_control* out);
+
+/* ---- context lifecycle ---- */
+
+/* Allocate the device state of one grid on `device`, build the mesh metrics
+   (domain/SMOD_mesh_manipulation.f90:14-178) and initialise the time control
+   (time_control/MOD_time_control.f90:70-151).  Replaces the allocations of main.f90:125-151. */
+int pcl_create(const pcl_solver_control* ctl, int device, pcl_ctx** out);
+int pcl_destroy(pcl_ctx* ctx);
+
+/* Copy the state in and out (reference layout, see top).  upload_state also makes it the
+   current solution of every rotation buffer. */
+int pcl_upload_state(pcl_ctx* ctx, const double* vars);
+int pcl_download_state(pcl_ctx* ctx, double* vars);
+
+/* ---- the hot path, one call per reference routine ---- */
+
+/* update_rank_boundaries (user_subroutines/SMOD_boundary_conditions.f90:17-56): on-device
+   ghost fill of the current solution; no halo exchange (one GPU holds the whole grid). */
+int pcl_update_rank_boundaries(pcl_ctx* ctx);
+
+/* solve_dimensional_split (solver/MOD_solve.f90:23-175): one attempted step with the current
+   dt: xi sweep, validity, eta sweep, validity.  *ierr = 1 accepted (the new solution is
+   current) or -1 rejected (the pre-step solution stays current, as after main.f90:221).
+   Updates the time control's CFL like update_max_CFL. */
+int pcl_solve_dimensional_split(pcl_ctx* ctx, int* ierr);
+
+/* solution = solution_old (main.f90:221).  A rejected attempt never overwrites the current
+   buffer, so this only has to exist for call-for-call parity; it is a no-op. */
+int pcl_restore_solution(pcl_ctx* ctx);
+
+/* integrate_source_term (solver/MOD_solve.f90:295-336) with the default source phi = 0
+   (user_subroutines/SMOD_source_function.f90:27): q + 0*dt, a no-op for finite q. */
+int pcl_integrate_source_term(pcl_ctx* ctx);
+
+/* ---- time control (time_control/MOD_time_control.f90), device resident ---- */
+int pcl_update_time(pcl_ctx* ctx, int step_valid);   /* updateTime :153-243 */
+int pcl_reset_cfl(pcl_ctx* ctx);                      /* reset_CFL :270-279 */
+int pcl_advance_snapshot_index(pcl_ctx* ctx);         /* advance_snapshot_index :254-260 */
+int pcl_set_dt(pcl_ctx* ctx, double dt);              /* host override of dt (tests) */
+int pcl_get_time(pcl_ctx* ctx, double* time);
+int pcl_get_dt(pcl_ctx* ctx, double* dt);             /* get_dt :290-297 */
+int pcl_get_previous_dt(pcl_ctx* ctx, double* dt);    /* get_previous_dt :299-306 */
+int pcl_get_cfl(pcl_ctx* ctx, double* cfl);           /* get_CFL :281-288 */
+int pcl_get_snapshot_index(pcl_ctx* ctx, int* idx);   /* get_snapshot_index :308-315 */
+int pcl_get_snapshot_time(pcl_ctx* ctx, int idx, double* t); /* snapshot_intervals(idx) */
+
+/* ---- the whole main loop on the device ---- */
+
+/* Run main.f90:193-283 (solve, reject/restore, ghost fill, updateTime, snapshot index,
+   reset_CFL) without a host round trip per step, in CUDA graphs of `chunk` attempts, until
+   time >= t_final, the accepted-step cap, an error, or max_attempts (0: no cap).  Every
+   attempt is logged on the device (pcl_get_step_log).  *stats may be NULL. */
+int pcl_advance(pcl_ctx* ctx, long long max_attempts, pcl_run_stats* stats);
+int pcl_get_stats(pcl_ctx* ctx, pcl_run_stats* stats);
+/* time_control%initialize again (MOD_time_control.f90:70-151) and clear the counters and the
+   step log: with pcl_upload_state, restarts a run on the same context. */
+int pcl_reset_time_control(pcl_ctx* ctx);
+/* Diagnostic: run `reps` device-loop attempts with a CUDA event around every kernel and return
+   the mean duration of each kernel kind in avg_ms[] (FP64: xi sweep, eta sweep, time control,
+   ghost fill; mixed: fused sweep, time control, ghost fill); *nkinds = entries written. */
+int pcl_profile_kernels(pcl_ctx* ctx, int reps, double* avg_ms, int* nkinds);
+/* Copy up to cap records of the device step log; *n = records logged so far. */
+int pcl_get_step_log(pcl_ctx* ctx, pcl_step_record* out, long long cap, long long* n);
+
+/* ---- utilities ---- */
+int pcl_synchronize(pcl_ctx* ctx);
+void* pcl_get_stream(pcl_ctx* ctx);                   /* the context's cudaStream_t */
+long long pcl_state_doubles(const pcl_ctx* ctx);      /* 3*(m_xi+4)*(m_eta+4) */
+long long pcl_device_bytes(const pcl_ctx* ctx);       /* device memory held by the context */
+int pcl_get_io_bytes(pcl_ctx* ctx, long long* h2d, long long* d2h); /* bytes copied so far */
+int pcl_host_alloc(void** ptr, long long bytes);      /* pinned host buffer */
+int pcl_host_free(void* ptr);
+const char* pcl_status_string(int status);
+int pcl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,681 @@
+// capi.cu -- the C ABI (include/paraclaws_b200.h): contexts, the control.in reader, and the
+// per-routine and whole-loop entry points.  Host arithmetic here (mesh tables, snapshot times)
+// is built without contraction (-ffp-contract=off) to round as the reference does.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../include/paraclaws_b200.h"
+#include "pcl_launch.h"
+#include "pcl_types.h"
+#include "pcl_mixed.h"
+
+using namespace pcl;
+
+struct pcl_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  pcl_solver_control cfg{};
+  GridDev g{};
+  Ctl* ctl_d = nullptr;
+  Ctl* ctl_h = nullptr;          // pinned mirror for reads
+  double* bufs_d = nullptr;      // 3 state buffers
+  double* tables_d = nullptr;    // row + column metric tables
+  double* staging_d = nullptr;   // AoS staging for upload/download
+  StepLogEntry* log_d = nullptr;
+  long long log_cap = 0;
+  size_t device_bytes = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_chunk = 0;
+  void* mixed = nullptr;         // mixed-precision workspace (pcl_mixed.h)
+  long long launches = 0;        // kernels launched by this context
+  long long graph_launches = 0;  // kernels in one launch of the captured graph
+  long long h2d_bytes = 0, d2h_bytes = 0;  // bytes copied across the host boundary
+};
+
+#define CK(call)                                       \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) {                           \
+      std::fprintf(stderr, "paraclaws_b200: %s: %s\n", #call, cudaGetErrorString(e_)); \
+      return PCL_ERR_CUDA;                             \
+    }                                                  \
+  } while (0)
+
+static int status_to_code(int st) {
+  if (st & kStatusNaN) return PCL_ERR_NAN;
+  if (st & kStatusNegDepth) return PCL_ERR_NEG_DEPTH;
+  if (st & kStatusTimeout) return PCL_ERR_TIMEOUT;
+  if (st & kStatusFatalDt) return PCL_ERR_FATAL_DT;
+  return PCL_OK;
+}
+
+extern "C" {
+
+int pcl_version(void) { return 100; }
+
+const char* pcl_status_string(int s) {
+  switch (s) {
+    case PCL_OK: return "ok";
+    case PCL_ERR_NAN: return "NaN in a flux Jacobian";
+    case PCL_ERR_NEG_DEPTH: return "negative water depth (complex eigenvalues)";
+    case PCL_ERR_TIMEOUT: return "device wait timed out";
+    case PCL_ERR_OOM: return "out of memory";
+    case PCL_ERR_BADARG: return "invalid argument";
+    case PCL_ERR_CUDA: return "CUDA error";
+    case PCL_ERR_FATAL_DT: return "time step control cannot continue (constant dt violated)";
+    case PCL_ERR_IO: return "cannot read control file";
+    case PCL_ERR_FULL: return "batch is full or over its memory budget";
+    default: return "unknown status";
+  }
+}
+
+void pcl_default_control(pcl_solver_control* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->num_equations = 3;
+  c->num_dimensions = 2;
+  c->num_ghost = 2;
+  c->num_aux = 10;
+  c->num_waves = 2;
+  c->t_start = 0.0;
+  c->t_final = 0.5;
+  c->number_of_snapshots = 5;
+  c->dt_initial = 1e-10;
+  c->adaptive_timestepping = 1;
+  c->cfl_limit = 0.1;
+  c->dt_min = 1e-10;
+  c->dt_max = 5e-5;
+  c->dt_max_growth_ratio = 1.2;
+  c->dt_min_shrink_ratio = 0.5;
+  c->higher_order_flux_correction = 0;
+  c->use_limiter = 1;
+  c->limiter_method = 1;
+  c->m_xi = c->m_eta = 21;
+  c->xi_min = -1.0; c->xi_max = 1.0; c->eta_min = -1.0; c->eta_max = 1.0;
+  c->bc_xi_lower = c->bc_xi_upper = c->bc_eta_lower = c->bc_eta_upper = 2;
+  c->precision_mode = PCL_PREC_FP64;
+  c->grav = (double)9.81f;  // examples/2D_dam_break/cartesian/SMOD_setup.f90:21
+  c->initial_condition = 1;
+  c->dam_radius = 0.5; c->dam_h_in = 2.0; c->dam_h_out = 1.0; c->dam_x0 = 0.0; c->dam_y0 = 0.0;
+  c->max_accepted_steps = 0;
+}
+
+// ---- list-directed reads (utility/MOD_IO.f90:61-94) ----
+static bool first_token(const std::string& rec, std::string& tok) {
+  size_t a = rec.find_first_not_of(" \t\r");
+  if (a == std::string::npos) return false;
+  size_t b = rec.find_first_of(" \t\r,/", a);
+  tok = rec.substr(a, b == std::string::npos ? std::string::npos : b - a);
+  return !tok.empty();
+}
+static bool parse_int(const std::string& t, int& v) {
+  char* e = nullptr;
+  long x = std::strtol(t.c_str(), &e, 10);
+  if (e == t.c_str() || *e) return false;
+  v = (int)x;
+  return true;
+}
+static bool parse_ll(const std::string& t, long long& v) {
+  char* e = nullptr;
+  long long x = std::strtoll(t.c_str(), &e, 10);
+  if (e == t.c_str() || *e) return false;
+  v = x;
+  return true;
+}
+static bool parse_real(std::string t, double& v) {
+  for (auto& ch : t)
+    if (ch == 'd' || ch == 'D') ch = 'e';
+  char* e = nullptr;
+  double x = std::strtod(t.c_str(), &e);
+  if (e == t.c_str() || *e) return false;
+  v = x;
+  return true;
+}
+static bool parse_logical(std::string t, int& v) {
+  if (!t.empty() && t[0] == '.') t = t.substr(1);
+  if (t.empty()) return false;
+  char ch = (char)std::toupper((unsigned char)t[0]);
+  if (ch == 'T') { v = 1; return true; }
+  if (ch == 'F') { v = 0; return true; }
+  return false;
+}
+static bool read_records(const char* path, std::vector<std::string>& toks) {
+  std::ifstream f(path);
+  if (!f) return false;
+  std::string line, tok;
+  while (std::getline(f, line))
+    if (first_token(line, tok)) toks.push_back(tok);
+  return true;
+}
+
+int pcl_read_solver_control(const char* control_in, const char* custom_in, pcl_solver_control* out) {
+  if (!control_in || !out) return PCL_ERR_BADARG;
+  pcl_default_control(out);
+  std::vector<std::string> t;
+  if (!read_records(control_in, t)) return PCL_ERR_IO;
+  if (t.size() < 28) return PCL_ERR_IO;
+  bool ok = true;
+  pcl_solver_control& c = *out;
+  ok &= parse_int(t[0], c.num_equations);
+  ok &= parse_int(t[1], c.num_dimensions);
+  ok &= parse_int(t[2], c.num_ghost);
+  ok &= parse_int(t[3], c.num_aux);
+  ok &= parse_int(t[4], c.num_waves);
+  ok &= parse_real(t[5], c.t_start);
+  ok &= parse_real(t[6], c.t_final);
+  ok &= parse_int(t[7], c.number_of_snapshots);
+  ok &= parse_real(t[8], c.dt_initial);
+  ok &= parse_logical(t[9], c.adaptive_timestepping);
+  ok &= parse_real(t[10], c.cfl_limit);
+  ok &= parse_real(t[11], c.dt_min);
+  ok &= parse_real(t[12], c.dt_max);
+  ok &= parse_real(t[13], c.dt_max_growth_ratio);
+  ok &= parse_real(t[14], c.dt_min_shrink_ratio);
+  ok &= parse_logical(t[15], c.higher_order_flux_correction);
+  ok &= parse_logical(t[16], c.use_limiter);
+  ok &= parse_int(t[17], c.limiter_method);
+  ok &= parse_int(t[18], c.m_xi);
+  ok &= parse_int(t[19], c.m_eta);
+  ok &= parse_real(t[20], c.xi_min);
+  ok &= parse_real(t[21], c.xi_max);
+  ok &= parse_real(t[22], c.eta_min);
+  ok &= parse_real(t[23], c.eta_max);
+  ok &= parse_int(t[24], c.bc_xi_lower);
+  ok &= parse_int(t[25], c.bc_xi_upper);
+  ok &= parse_int(t[26], c.bc_eta_lower);
+  ok &= parse_int(t[27], c.bc_eta_upper);
+  if (!ok) return PCL_ERR_IO;
+  if (custom_in) {
+    std::vector<std::string> u;
+    if (read_records(custom_in, u) && u.size() >= 9) {
+      ok &= parse_ll(u[0], c.max_accepted_steps);
+      ok &= parse_int(u[1], c.precision_mode);
+      ok &= parse_real(u[2], c.grav);
+      ok &= parse_int(u[3], c.initial_condition);
+      ok &= parse_real(u[4], c.dam_radius);
+      ok &= parse_real(u[5], c.dam_h_in);
+      ok &= parse_real(u[6], c.dam_h_out);
+      ok &= parse_real(u[7], c.dam_x0);
+      ok &= parse_real(u[8], c.dam_y0);
+      if (!ok) return PCL_ERR_IO;
+    }
+  }
+  return PCL_OK;
+}
+
+static int validate(const pcl_solver_control* c) {
+  if (c->num_equations != 3 || c->num_waves != 2 || c->num_ghost != 2) return PCL_ERR_BADARG;
+  if (c->m_xi < 2 || c->m_eta < 2) return PCL_ERR_BADARG;
+  const int bcs[4] = {c->bc_xi_lower, c->bc_xi_upper, c->bc_eta_lower, c->bc_eta_upper};
+  for (int k = 0; k < 4; ++k)
+    if (bcs[k] < 1 || bcs[k] > 3) return PCL_ERR_BADARG;
+  if (c->higher_order_flux_correction && c->use_limiter && (c->limiter_method < 1 || c->limiter_method > 4))
+    return PCL_ERR_BADARG;
+  if (c->dt_min > c->dt_max) return PCL_ERR_BADARG;
+  if (c->precision_mode != PCL_PREC_FP64 && c->precision_mode != PCL_PREC_MIXED) return PCL_ERR_BADARG;
+  if (c->number_of_snapshots > kMaxSnapshots) return PCL_ERR_BADARG;
+  if (!(c->xi_max > c->xi_min) || !(c->eta_max > c->eta_min)) return PCL_ERR_BADARG;
+  return PCL_OK;
+}
+
+// mesh tables in the reference's operation order (domain/SMOD_mesh_manipulation.f90)
+static void build_tables(const pcl_solver_control* c, double dxi, double deta, std::vector<double>& rowm,
+                         std::vector<double>& colm) {
+  const int ni = c->m_xi + 4, nj = c->m_eta + 4;
+  rowm.assign((size_t)nj * kRowMetrics, 0.0);
+  colm.assign((size_t)ni * kColMetrics, 0.0);
+  for (int j = -1; j <= c->m_eta + 2; ++j) {
+    const double e1 = c->eta_min + (double)(j - 1) * deta;  // eta_corner(1) :43
+    const double e3 = e1 + deta;                            // eta_corner(3) :45
+    double* r = &rowm[(size_t)(j + 1) * kRowMetrics];
+    r[0] = 0.5 * (e1 + e1);
+    r[1] = 0.5 * (e3 + e3);
+    r[2] = std::fabs(e3 - e1) / deta;  // length_ratio_xi :147-153, NORM2([0, dy]) = |dy|
+    r[3] = c->eta_min + (double)(j - 1) * deta + deta / 2;  // eta centre :51
+  }
+  for (int i = -1; i <= c->m_xi + 2; ++i) {
+    const double c1 = c->xi_min + (double)(i - 1) * dxi;  // xi_corner(1) :36
+    const double c2 = c1 + dxi;                            // xi_corner(2) :37
+    double* r = &colm[(size_t)(i + 1) * kColMetrics];
+    r[0] = c1 - c2;
+    r[1] = c2 - c1;
+    r[2] = std::fabs(c2 - c1) / dxi;  // length_ratio_eta :156-162
+    r[3] = c->xi_min + (double)(i - 1) * dxi + dxi / 2;  // xi centre :50
+  }
+}
+
+// time_control%initialize (MOD_time_control.f90:70-151)
+static void init_ctl(const pcl_solver_control* c, Ctl& t) {
+  std::memset(&t, 0, sizeof(t));
+  t.time_initial = c->t_start;
+  t.time_final = c->t_final;
+  t.time = c->t_start;
+  t.dt = c->dt_initial;
+  t.dt_previous = c->dt_initial;
+  t.dt_max = c->dt_max;
+  t.dt_min = c->dt_min;
+  t.adaptive = c->adaptive_timestepping ? 1 : 0;
+  t.n_snapshots = c->number_of_snapshots < 1 ? 1 : c->number_of_snapshots;
+  const double si = (t.time_final - t.time_initial) / t.n_snapshots;
+  for (int i = 1; i <= t.n_snapshots; ++i) t.snap_times[i - 1] = t.time_initial + i * si;
+  t.snap_times[t.n_snapshots - 1] = t.time_final;
+  t.snapshot_index = 1;
+  t.CFL = 0.0;
+  t.CFL_previous_timestep = 0.0;
+  t.CFL_target = c->cfl_limit;
+  t.time_precision = 0.01;
+  t.growth = c->dt_max_growth_ratio;
+  t.shrink = c->dt_min_shrink_ratio;
+  t.emergency = 0.25;
+  t.cur = 0;
+  t.max_accepted = c->max_accepted_steps;
+}
+
+static void free_ctx(pcl_ctx* x) {
+  if (!x) return;
+  if (x->graph) cudaGraphExecDestroy(x->graph);
+  if (x->mixed) mixed_free(x->mixed);
+  cudaFree(x->bufs_d);
+  cudaFree(x->tables_d);
+  cudaFree(x->staging_d);
+  cudaFree(x->ctl_d);
+  cudaFree(x->log_d);
+  if (x->ctl_h) cudaFreeHost(x->ctl_h);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+}
+
+int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
+  if (!c || !out) return PCL_ERR_BADARG;
+  *out = nullptr;
+  int v = validate(c);
+  if (v != PCL_OK) return v;
+  CK(cudaSetDevice(device));
+  pcl_ctx* x = new pcl_ctx();
+  x->device = device;
+  x->cfg = *c;
+  auto fail = [&](int code) {
+    free_ctx(x);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PCL_ERR_CUDA);
+  const int ni = c->m_xi + 4, nj = c->m_eta + 4;
+  const int pitch = (ni + 31) / 32 * 32;
+  const long long plane = (long long)pitch * nj;
+  const size_t buf_bytes = sizeof(double) * 3 * 3 * (size_t)plane;
+  const double dxi = (c->xi_max - c->xi_min) / c->m_xi;     // :28
+  const double deta = (c->eta_max - c->eta_min) / c->m_eta;  // :29
+  std::vector<double> rowm, colm;
+  build_tables(c, dxi, deta, rowm, colm);
+  const size_t tab_bytes = sizeof(double) * (rowm.size() + colm.size());
+  const size_t stg_bytes = sizeof(double) * 3 * (size_t)ni * nj;
+  x->log_cap = 1 << 16;
+  if (cudaMalloc(&x->bufs_d, buf_bytes) != cudaSuccess) return fail(PCL_ERR_OOM);
+  if (cudaMalloc(&x->tables_d, tab_bytes) != cudaSuccess) return fail(PCL_ERR_OOM);
+  if (cudaMalloc(&x->staging_d, stg_bytes) != cudaSuccess) return fail(PCL_ERR_OOM);
+  if (cudaMalloc(&x->ctl_d, sizeof(Ctl)) != cudaSuccess) return fail(PCL_ERR_OOM);
+  if (cudaMalloc(&x->log_d, sizeof(StepLogEntry) * x->log_cap) != cudaSuccess) return fail(PCL_ERR_OOM);
+  if (cudaMallocHost(&x->ctl_h, sizeof(Ctl)) != cudaSuccess) return fail(PCL_ERR_OOM);
+  x->device_bytes = buf_bytes + tab_bytes + stg_bytes + sizeof(Ctl) + sizeof(StepLogEntry) * x->log_cap;
+  if (cudaMemsetAsync(x->bufs_d, 0, buf_bytes, x->stream) != cudaSuccess) return fail(PCL_ERR_CUDA);
+  if (cudaMemcpyAsync(x->tables_d, rowm.data(), sizeof(double) * rowm.size(), cudaMemcpyHostToDevice, x->stream) != cudaSuccess)
+    return fail(PCL_ERR_CUDA);
+  if (cudaMemcpyAsync(x->tables_d + rowm.size(), colm.data(), sizeof(double) * colm.size(), cudaMemcpyHostToDevice,
+                      x->stream) != cudaSuccess)
+    return fail(PCL_ERR_CUDA);
+  init_ctl(c, *x->ctl_h);
+  x->ctl_h->log = x->log_d;
+  x->ctl_h->log_cap = x->log_cap;
+  if (cudaMemcpyAsync(x->ctl_d, x->ctl_h, sizeof(Ctl), cudaMemcpyHostToDevice, x->stream) != cudaSuccess)
+    return fail(PCL_ERR_CUDA);
+  GridDev& g = x->g;
+  g.state = x->bufs_d;
+  g.bufstride = 3 * plane;
+  g.rowm = x->tables_d;
+  g.colm = x->tables_d + rowm.size();
+  g.ctl = x->ctl_d;
+  g.plane = plane;
+  g.mx = c->m_xi;
+  g.my = c->m_eta;
+  g.pitch = pitch;
+  g.bc[0] = c->bc_xi_lower; g.bc[1] = c->bc_xi_upper; g.bc[2] = c->bc_eta_lower; g.bc[3] = c->bc_eta_upper;
+  g.second_order = c->higher_order_flux_correction ? 1 : 0;
+  g.limiter = c->use_limiter ? c->limiter_method : 0;
+  g.dxi = dxi;
+  g.deta = deta;
+  g.area_scale = dxi * deta;  // d_xi*d_eta (SMOD_mesh_manipulation.f90:173)
+  g.grav = c->grav;
+  if (c->precision_mode == PCL_PREC_MIXED) {
+    int r = mixed_create(g, x->stream, &x->mixed);
+    if (r != PCL_OK) return fail(r);
+  }
+  launch_timectl(g, kOpInit, 0, 0.0, x->stream);
+  if (cudaStreamSynchronize(x->stream) != cudaSuccess) return fail(PCL_ERR_CUDA);
+  if (cudaGetLastError() != cudaSuccess) return fail(PCL_ERR_CUDA);
+  *out = x;
+  return PCL_OK;
+}
+
+int pcl_destroy(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  cudaSetDevice(x->device);
+  cudaStreamSynchronize(x->stream);
+  free_ctx(x);
+  return PCL_OK;
+}
+
+long long pcl_state_doubles(const pcl_ctx* x) { return x ? 3LL * (x->cfg.m_xi + 4) * (x->cfg.m_eta + 4) : 0; }
+long long pcl_device_bytes(const pcl_ctx* x) { return x ? (long long)x->device_bytes : 0; }
+void* pcl_get_stream(pcl_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+// the control block without its snapshot table (which only the host writes)
+static const size_t kCtlHotBytes = offsetof(Ctl, snap_times);
+
+static int read_ctl(pcl_ctx* x) {
+  x->d2h_bytes += (long long)kCtlHotBytes;
+  CK(cudaMemcpyAsync(x->ctl_h, x->ctl_d, kCtlHotBytes, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return PCL_OK;
+}
+
+static int check_launch(pcl_ctx* x) {
+  CK(cudaGetLastError());
+  return PCL_OK;
+}
+
+int pcl_synchronize(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  CK(cudaStreamSynchronize(x->stream));
+  int r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  return status_to_code(x->ctl_h->status);
+}
+
+int pcl_upload_state(pcl_ctx* x, const double* vars) {
+  if (!x || !vars) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  x->h2d_bytes += (long long)sizeof(double) * pcl_state_doubles(x);
+  CK(cudaMemcpyAsync(x->staging_d, vars, sizeof(double) * pcl_state_doubles(x), cudaMemcpyHostToDevice, x->stream));
+  launch_upload(x->g, x->staging_d, x->stream);
+  int r = check_launch(x);
+  if (r != PCL_OK) return r;
+  CK(cudaStreamSynchronize(x->stream));
+  return PCL_OK;
+}
+
+int pcl_download_state(pcl_ctx* x, double* vars) {
+  if (!x || !vars) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  launch_download(x->g, x->staging_d, x->stream);
+  int r = check_launch(x);
+  if (r != PCL_OK) return r;
+  x->d2h_bytes += (long long)sizeof(double) * pcl_state_doubles(x);
+  CK(cudaMemcpyAsync(vars, x->staging_d, sizeof(double) * pcl_state_doubles(x), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return PCL_OK;
+}
+
+int pcl_update_rank_boundaries(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  launch_ghost(x->g, 1, x->stream);
+  x->launches += 1;
+  return check_launch(x);
+}
+
+static int sweep_kernels(const pcl_ctx* x) { return x->cfg.precision_mode == PCL_PREC_MIXED ? 1 : 2; }
+
+static void launch_sweeps(pcl_ctx* x) {
+  if (x->cfg.precision_mode == PCL_PREC_MIXED)
+    launch_sweeps_mixed(x->g, x->mixed, x->stream);
+  else
+    launch_sweeps_fp64(x->g, x->stream);
+  x->launches += sweep_kernels(x);
+}
+
+int pcl_solve_dimensional_split(pcl_ctx* x, int* ierr) {
+  if (!x || !ierr) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  launch_sweeps(x);
+  launch_timectl(x->g, kOpFinalizeSolve, 0, 0.0, x->stream);
+  x->launches += 1;
+  int r = check_launch(x);
+  if (r != PCL_OK) return r;
+  r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  *ierr = x->ctl_h->ierr;
+  return status_to_code(x->ctl_h->status);
+}
+
+int pcl_restore_solution(pcl_ctx* x) { return x ? PCL_OK : PCL_ERR_BADARG; }
+int pcl_integrate_source_term(pcl_ctx* x) { return x ? PCL_OK : PCL_ERR_BADARG; }
+
+static int timeop(pcl_ctx* x, int op, int arg, double value) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  launch_timectl(x->g, op, arg, value, x->stream);
+  x->launches += 1;
+  return check_launch(x);
+}
+
+int pcl_update_time(pcl_ctx* x, int step_valid) {
+  int r = timeop(x, kOpUpdateTime, step_valid ? 1 : 0, 0.0);
+  if (r != PCL_OK) return r;
+  r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  return status_to_code(x->ctl_h->status);
+}
+int pcl_reset_cfl(pcl_ctx* x) { return timeop(x, kOpResetCFL, 0, 0.0); }
+int pcl_advance_snapshot_index(pcl_ctx* x) { return timeop(x, kOpAdvanceSnapshot, 0, 0.0); }
+int pcl_set_dt(pcl_ctx* x, double dt) { return timeop(x, kOpSetDt, 0, dt); }
+
+#define GETTER(name, type, expr)                 \
+  int name(pcl_ctx* x, type* v) {                \
+    if (!x || !v) return PCL_ERR_BADARG;         \
+    CK(cudaSetDevice(x->device));                \
+    int r = read_ctl(x);                         \
+    if (r != PCL_OK) return r;                   \
+    *v = (expr);                                 \
+    return PCL_OK;                               \
+  }
+GETTER(pcl_get_time, double, x->ctl_h->time)
+GETTER(pcl_get_dt, double, x->ctl_h->dt)
+GETTER(pcl_get_previous_dt, double, x->ctl_h->dt_previous)
+GETTER(pcl_get_cfl, double, x->ctl_h->CFL)
+GETTER(pcl_get_snapshot_index, int, x->ctl_h->snapshot_index)
+#undef GETTER
+
+int pcl_get_snapshot_time(pcl_ctx* x, int idx, double* t) {
+  if (!x || !t) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  int r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  if (idx < 1 || idx > x->ctl_h->n_snapshots) return PCL_ERR_BADARG;
+  *t = x->ctl_h->snap_times[idx - 1];
+  return PCL_OK;
+}
+
+static void fill_stats(const Ctl& c, long long launches, pcl_run_stats* s) {
+  s->launches = launches;
+  s->attempts = c.attempts;
+  s->accepted = c.accepted;
+  s->rejected = c.attempts - c.accepted;
+  s->time = c.time;
+  s->dt = c.dt;
+  s->dt_previous = c.dt_previous;
+  s->cfl = c.CFL;
+  s->snapshot_index = c.snapshot_index;
+  s->done = c.done;
+  s->status = status_to_code(c.status);
+  s->last_ierr = c.ierr;
+}
+
+int pcl_get_stats(pcl_ctx* x, pcl_run_stats* s) {
+  if (!x || !s) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  int r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  fill_stats(*x->ctl_h, x->launches, s);
+  return PCL_OK;
+}
+
+static void enqueue_attempt(pcl_ctx* x) {
+  launch_sweeps(x);
+  launch_timectl(x->g, kOpFullStep, 0, 0.0, x->stream);
+  launch_ghost(x->g, 0, x->stream);
+  x->launches += 2;
+}
+
+static int build_graph(pcl_ctx* x, int chunk) {
+  if (x->graph && x->graph_chunk == chunk) return PCL_OK;
+  if (x->graph) {
+    cudaGraphExecDestroy(x->graph);
+    x->graph = nullptr;
+  }
+  cudaGraph_t gr;
+  const long long before = x->launches;
+  CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < chunk; ++k) enqueue_attempt(x);
+  CK(cudaStreamEndCapture(x->stream, &gr));
+  x->graph_launches = x->launches - before;  // kernels per graph launch
+  x->launches = before;
+  cudaError_t e = cudaGraphInstantiate(&x->graph, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) return PCL_ERR_CUDA;
+  x->graph_chunk = chunk;
+  return PCL_OK;
+}
+
+int pcl_advance(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  const int chunk = 32;
+  int r = build_graph(x, chunk);
+  if (r != PCL_OK) return r;
+  r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  const long long start = x->ctl_h->attempts;
+  timeop(x, kOpInit, 0, 0.0);  // refresh done / dt ratios after any host-side change
+  r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  while (!x->ctl_h->done) {
+    const long long doneatt = x->ctl_h->attempts - start;
+    if (max_attempts > 0 && doneatt >= max_attempts) break;
+    if (max_attempts > 0 && max_attempts - doneatt < chunk) {
+      for (long long k = doneatt; k < max_attempts; ++k) enqueue_attempt(x);
+    } else {
+      CK(cudaGraphLaunch(x->graph, x->stream));
+      x->launches += x->graph_launches;
+    }
+    r = check_launch(x);
+    if (r != PCL_OK) return r;
+    r = read_ctl(x);
+    if (r != PCL_OK) return r;
+  }
+  if (stats) fill_stats(*x->ctl_h, x->launches, stats);
+  return status_to_code(x->ctl_h->status);
+}
+
+int pcl_reset_time_control(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  CK(cudaStreamSynchronize(x->stream));
+  int r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  const int cur = x->ctl_h->cur;
+  init_ctl(&x->cfg, *x->ctl_h);
+  x->ctl_h->cur = cur;
+  x->ctl_h->log = x->log_d;
+  x->ctl_h->log_cap = x->log_cap;
+  CK(cudaMemcpyAsync(x->ctl_d, x->ctl_h, sizeof(Ctl), cudaMemcpyHostToDevice, x->stream));
+  launch_timectl(x->g, kOpInit, 0, 0.0, x->stream);
+  x->launches += 1;
+  CK(cudaStreamSynchronize(x->stream));
+  return check_launch(x);
+}
+
+int pcl_profile_kernels(pcl_ctx* x, int reps, double* avg_ms, int* nkinds) {
+  if (!x || !avg_ms || reps < 1) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  const int nk = sweep_kernels(x) + 2;
+  cudaEvent_t ev[6];
+  for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int r = 0; r < reps; ++r) {
+    int e = 0;
+    CK(cudaEventRecord(ev[e++], x->stream));
+    if (x->cfg.precision_mode == PCL_PREC_MIXED) {
+      launch_sweeps_mixed(x->g, x->mixed, x->stream);
+      CK(cudaEventRecord(ev[e++], x->stream));
+    } else {
+      launch_xsweep_fp64(x->g, x->stream);
+      CK(cudaEventRecord(ev[e++], x->stream));
+      launch_ysweep_fp64(x->g, x->stream);
+      CK(cudaEventRecord(ev[e++], x->stream));
+    }
+    launch_timectl(x->g, kOpFullStep, 0, 0.0, x->stream);
+    CK(cudaEventRecord(ev[e++], x->stream));
+    launch_ghost(x->g, 0, x->stream);
+    CK(cudaEventRecord(ev[e++], x->stream));
+    x->launches += nk;
+    CK(cudaEventSynchronize(ev[e - 1]));
+    for (int k = 0; k + 1 < e; ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      acc[k] += ms;
+    }
+  }
+  for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < nk; ++k) avg_ms[k] = acc[k] / reps;
+  if (nkinds) *nkinds = nk;
+  return check_launch(x);
+}
+
+int pcl_get_step_log(pcl_ctx* x, pcl_step_record* out, long long cap, long long* n) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  int r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  const long long len = x->ctl_h->log_len;
+  if (n) *n = len;
+  const long long m = len < cap ? len : cap;
+  if (out && m > 0) {
+    std::vector<StepLogEntry> tmp((size_t)m);
+    CK(cudaMemcpy(tmp.data(), x->log_d, sizeof(StepLogEntry) * m, cudaMemcpyDeviceToHost));
+    for (long long k = 0; k < m; ++k) {
+      out[k].dt = tmp[k].dt;
+      out[k].cfl = tmp[k].cfl;
+      out[k].time = tmp[k].time;
+      out[k].dt_next = tmp[k].dt_next;
+      out[k].ierr = tmp[k].ierr;
+      out[k].snapshot_index = tmp[k].snapshot_index;
+    }
+  }
+  return PCL_OK;
+}
+
+int pcl_get_io_bytes(pcl_ctx* x, long long* h2d, long long* d2h) {
+  if (!x) return PCL_ERR_BADARG;
+  if (h2d) *h2d = x->h2d_bytes;
+  if (d2h) *d2h = x->d2h_bytes;
+  return PCL_OK;
+}
+
+int pcl_host_alloc(void** p, long long bytes) {
+  if (!p || bytes <= 0) return PCL_ERR_BADARG;
+  if (cudaMallocHost(p, (size_t)bytes) != cudaSuccess) return PCL_ERR_OOM;
+  return PCL_OK;
+}
+int pcl_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+  return PCL_OK;
+}
+
+}  // extern "C"

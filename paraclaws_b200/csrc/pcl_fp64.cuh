@@ -1,0 +1,155 @@
+// pcl_fp64.cuh -- FP64 arithmetic of the wave-propagation step, bit-compatible with the
+// reference's operation order.  Every translation unit that includes this header is compiled
+// with --fmad=false so no multiply-add is contracted (the reference's rounding points are kept).
+//
+// Sweep direction DIR: 0 = xi sweep (normal momentum hu), 1 = eta sweep (normal momentum hv).
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "pcl_types.h"
+
+namespace pcl {
+
+// Flux Jacobian of the shallow-water equation module and its product with q
+// (examples/2D_dam_break/cartesian/SMOD_jakobian.f90:44-53; utility/SMOD_matrix_operations.f90:22
+// through BLAS dgemv 'N', which accumulates y = ((0 + q1*J(:,1)) + q2*J(:,2)) + q3*J(:,3)).
+// Non-constant Jacobian entries (both sweeps share them):
+//   jn = -(n*n)/(h*h) + g*h,  d2 = (2n)/h,  jt = -(hu*hv)/(h*h),  d4 = hv/h,  d5 = hu/h
+// Flux components in (h, hu, hv) order:
+//   xi : (hu, h*jn + hu*d2, (h*jt + hu*d4) + hv*d5)
+//   eta: (hv, (h*jt + hu*d4) + hv*d5, h*jn + hv*d2)
+// Wave speed bound of the cell: the eigenvalues of J are u-c, u, u+c with u = n/h and
+// c = sqrt(g*h), whose largest magnitude is fl(|u| + c) in round-to-nearest
+// (solver/SMOD_approximate_Riemann_solvers.f90:186-190 takes maxval of |eig| over both cells).
+struct CellFlux {
+  double f0, f1, f2, s;
+};
+
+template <int DIR>
+__device__ __forceinline__ CellFlux cell_flux(double h, double hu, double hv, double g, int* bad) {
+  const double n = DIR == 0 ? hu : hv;
+  const double hh = h * h;
+  const double d1 = (n * n) / hh;
+  const double d3 = (hu * hv) / hh;
+  const double d4 = hv / h;
+  const double d5 = hu / h;
+  const double un = DIR == 0 ? d5 : d4;
+  // (2n)/h == 2*(n/h) exactly unless n/h is subnormal (scaling by 2 commutes with rounding)
+  const double d2 = fabs(un) >= 0x1p-1000 ? 2.0 * un : (2.0 * n) / h;
+  const double gh = g * h;
+  const double jn = -d1 + gh;
+  const double jt = -d3;
+  CellFlux c;
+  c.f0 = n;
+  const double fnorm = h * jn + n * d2;
+  const double ftran = (h * jt + hu * d4) + hv * d5;
+  c.f1 = DIR == 0 ? fnorm : ftran;
+  c.f2 = DIR == 0 ? ftran : fnorm;
+  c.s = fabs(un) + sqrt(gh);
+  // getJakobi's NaN trap (SMOD_jakobian.f90:55-70) and dgeev's complex-eigenvalue abort
+  // (utility/SMOD_eigenvalue_problem.f90:72-83, h < 0) become status bits.
+  if (isnan(jn) || isnan(d2) || isnan(jt) || isnan(d4) || isnan(d5)) *bad |= kStatusNaN;
+  if (h < 0.0) *bad |= kStatusNegDepth;
+  return c;
+}
+
+// HLL two-wave solve at one interface (SMOD_approximate_Riemann_solvers.f90:189-224):
+// s2 = max(sL, sR), s1 = -s2; if |s1| > eps and |s2| > eps:
+//   q* = (((fR - fL) - s2*qR) + s1*qL) / ((eps + s1) - s2),  W1 = q* - qL,  W2 = qR - q*
+// else lambda = 0 and W = 0.  Returns s2 (0 for the degenerate interface).
+struct Waves {
+  double w1[3], w2[3];
+};
+
+__device__ __forceinline__ double hll(const double qL[3], const CellFlux& fL, const double qR[3],
+                                      const CellFlux& fR, Waves& W) {
+  const double smax = fmax(fL.s, fR.s);
+  const double s1 = -smax;
+  if (fabs(s1) > kUdPrecision && fabs(smax) > kUdPrecision) {
+    const double den = (kUdPrecision + s1) - smax;
+    const double fl[3] = {fL.f0, fL.f1, fL.f2};
+    const double fr[3] = {fR.f0, fR.f1, fR.f2};
+#pragma unroll
+    for (int me = 0; me < 3; ++me) {
+      const double qs = (((fr[me] - fl[me]) - smax * qR[me]) + s1 * qL[me]) / den;
+      W.w1[me] = qs - qL[me];
+      W.w2[me] = qR[me] - qs;
+    }
+    return smax;
+  }
+#pragma unroll
+  for (int me = 0; me < 3; ++me) {
+    W.w1[me] = 0.0;
+    W.w2[me] = 0.0;
+  }
+  return 0.0;
+}
+
+// limiter function phi(theta) by code (solver/MOD_flux_correction.f90:101-112)
+template <int LIM>
+__device__ __forceinline__ double limiter_phi(double r) {
+  if (LIM == 1) return fmax(0.0, fmin(1.0, r));
+  if (LIM == 2) return fmax(fmax(0.0, fmin(1.0, 2.0 * r)), fmin(2.0, r));
+  if (LIM == 3) return (r + fabs(r)) / (1.0 + fabs(r));
+  return fmax(0.0, fmin(fmin((1.0 + r) / 2.0, 2.0), 2.0 * r));
+}
+
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+}
+
+// Limited wave for one family p at interface k (MOD_flux_correction.f90:74-123).  All three
+// waves are the unlimited ones: the reference's carried wnorm2r is the dot product of the
+// original waves at k and k+1, taken before wave k is limited in place.
+//   upstream = lambda_p > 0 ? W_{k-1}.W_k : W_k.W_{k+1};  theta = upstream / |W_k|^2
+//   W~ = |W_k|^2 <= eps ? W_k : phi(theta) * W_k
+template <int LIM>
+__device__ __forceinline__ void limit_wave(const double wm[3], const double w[3], const double wp[3],
+                                           bool lambda_pos, double out[3]) {
+  const double wn2 = dot3(w, w);
+  if (fabs(wn2) <= kUdPrecision) {
+    out[0] = w[0];
+    out[1] = w[1];
+    out[2] = w[2];
+    return;
+  }
+  const double up = lambda_pos ? dot3(wm, w) : dot3(w, wp);
+  const double phi = limiter_phi<LIM>(up / wn2);
+  out[0] = phi * w[0];
+  out[1] = phi * w[1];
+  out[2] = phi * w[2];
+}
+
+// Correction coefficient of one interface, the same for both waves because |s1| = |s2|
+// (MOD_flux_correction.f90:162-165): (0.5*|l|) * (1 - (|l|*dt/delta) / (0.5*(kap_{k-1}+kap_k)))
+__device__ __forceinline__ double corr_coef(double s2, double dtod, double kap_l, double kap_r) {
+  if (s2 == 0.0) return 0.0;
+  const double kb = 0.5 * (kap_l + kap_r);
+  return (0.5 * s2) * (1.0 - (s2 * dtod) / kb);
+}
+
+// Capacity kappa(i,j) of the uniform identity-mapped grid: the shoelace area
+// (domain/SMOD_mesh_manipulation.f90:165-173) reduces to (p1*d + p3*d') / (d_xi*d_eta) with
+// p1 = 0.5*(e1+e1), p3 = 0.5*(e3+e3) per row and d = c1-c2, d' = c2-c1 per column; the two
+// vanishing shoelace terms are signed zeros that leave a non-zero sum unchanged.
+__device__ __forceinline__ double capacity(const double* rowm, const double* colm, int i, int j,
+                                           double area_scale) {
+  const double p1 = __ldg(rowm + (j + 1) * kRowMetrics + 0);
+  const double p3 = __ldg(rowm + (j + 1) * kRowMetrics + 1);
+  const double d = __ldg(colm + (i + 1) * kColMetrics + 0);
+  const double dp = __ldg(colm + (i + 1) * kColMetrics + 1);
+  return (p1 * d + p3 * dp) / area_scale;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  if (v > 0.0) atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+}  // namespace pcl

@@ -1,0 +1,164 @@
+"""FP64 CUDA path vs the CPU oracle: bit-identical state, dt sequence and accept/reject flags.
+
+The comparison is exact (numpy array_equal: IEEE equality, so -0 == +0); the FP64 path
+reproduces the oracle's operation order without contraction.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from paraclaws_b200 import control as ctl
+from paraclaws_b200 import ic
+from paraclaws_b200.solver import Solver, run_host_loop
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(control, custom=None):
+    from oracle.oracle import Oracle
+    return Solver(control, custom), Oracle(control, custom)
+
+
+def _start(s, o, q):
+    s.upload(q)
+    s.update_rank_boundaries()
+    o.set_state(q)
+    o.update_rank_boundaries()
+
+
+def _assert_state_equal(a, b, what=""):
+    if not np.array_equal(a, b):
+        d = np.abs(a - b)
+        idx = np.unravel_index(np.argmax(d), d.shape)
+        raise AssertionError(f"{what}: {np.count_nonzero(d)} values differ, max {d.max():.3e} at {idx}: "
+                             f"gpu {a[idx]!r} oracle {b[idx]!r}")
+
+
+@pytest.mark.parametrize("mx,my", [(16, 16), (37, 23), (5, 70), (200, 200), (257, 131)])
+@pytest.mark.parametrize("limiter", [1, 4])
+def test_one_attempt_matches_oracle(pcl, oracle_lib, mx, my, limiter):
+    c = ctl.dam_break_control(mx, limiter=limiter)
+    c = dataclasses.replace(c, m_eta=my, initial_timestep=2e-3)
+    s, o = _pair(c)
+    q = ic.gaussian_bumps(mx, my, seed=7)
+    q[..., 1] = 0.3 * np.sin(np.arange(q.shape[1]))[None, :]   # non-zero momenta
+    q[..., 2] = -0.2 * np.cos(np.arange(q.shape[0]))[:, None]
+    _start(s, o, q)
+    _assert_state_equal(s.download(), o.state(), "after ghost fill")
+    ierr = s.solve_dimensional_split()
+    st, ierr_o = o.solve_dimensional_split()
+    assert st == 0
+    assert ierr == ierr_o == 1
+    assert s.cfl == o.time_state()["cfl"]
+    _assert_state_equal(s.download(), o.state(), "after one attempt")
+
+
+@pytest.mark.parametrize("limiter", [1, 2, 3, 4])
+@pytest.mark.parametrize("bc", [1, 2, 3])
+def test_full_run_small(pcl, oracle_lib, limiter, bc):
+    c = ctl.dam_break_control(40, limiter=limiter, bc=bc, time_final=0.1)
+    s, o = _pair(c)
+    q = ic.circular_dam(40, 40)
+    _start(s, o, q)
+    st = s.advance()
+    log_o = o.run()
+    assert log_o.status == 0 and st.status == 0
+    lg = s.step_log()
+    assert len(lg.dt) == len(log_o.dt)
+    assert np.array_equal(lg.dt, log_o.dt)
+    assert np.array_equal(lg.ierr, log_o.ierr)
+    assert np.array_equal(lg.cfl, log_o.cfl)
+    assert np.array_equal(lg.time, log_o.time)
+    _assert_state_equal(s.download(), o.state(), "final state")
+
+
+def test_dam_break_200_to_t05(pcl, oracle_lib):
+    """The plain small workload: 200^2 dam break, MC limiter, CFL 0.9, to t = 0.5."""
+    c = ctl.dam_break_control(200, limiter=4, bc=2, time_final=0.5)
+    s, o = _pair(c)
+    q = ic.circular_dam(200, 200)
+    _start(s, o, q)
+    st = s.advance()
+    log_o = o.run()
+    lg = s.step_log()
+    assert st.accepted == log_o.accepted and st.time == 0.5
+    assert np.array_equal(lg.dt, log_o.dt)
+    assert np.array_equal(lg.ierr, log_o.ierr)
+    _assert_state_equal(s.download(), o.state(), "t=0.5")
+
+
+def test_first_order_and_unlimited(pcl, oracle_lib):
+    for over in (dict(add_higher_order_flux_correction=False), dict(use_limtiter=False)):
+        c = dataclasses.replace(ctl.dam_break_control(33, time_final=0.05), **over)
+        s, o = _pair(c)
+        q = ic.circular_dam(33, 33)
+        _start(s, o, q)
+        s.advance()
+        log_o = o.run()
+        assert np.array_equal(s.step_log().dt, log_o.dt)
+        _assert_state_equal(s.download(), o.state(), str(over))
+
+
+def test_host_loop_equals_device_loop(pcl, oracle_lib):
+    c = ctl.dam_break_control(48, limiter=1, time_final=0.05)
+    q = ic.circular_dam(48, 48)
+    a = Solver(c)
+    a.upload(q)
+    a.update_rank_boundaries()
+    la = run_host_loop(a)
+    b = Solver(c)
+    b.upload(q)
+    b.update_rank_boundaries()
+    b.advance()
+    lb = b.step_log()
+    assert np.array_equal(la.dt, lb.dt)
+    assert np.array_equal(la.ierr, lb.ierr)
+    assert np.array_equal(a.download(), b.download())
+
+
+def test_rejected_step_restores_and_shrinks_dt(pcl, oracle_lib):
+    """A dt far above the CFL limit is rejected after the xi sweep: state untouched, dt*0.25."""
+    c = dataclasses.replace(ctl.dam_break_control(64, limiter=4), initial_timestep=0.02)
+    s, o = _pair(c)
+    q = ic.circular_dam(64, 64)
+    _start(s, o, q)
+    before = s.download()
+    ierr = s.solve_dimensional_split()
+    assert ierr == -1
+    s.update_time(False)
+    s.reset_cfl()
+    assert s.dt == 0.25 * 0.02  # emergency_shrink_ratio (below dt_max = 1e-2, so unclamped)
+    assert np.array_equal(s.download(), before)
+    st = s.advance()
+    log_o = o.run()
+    lg = s.step_log()
+    assert (log_o.ierr < 0).sum() >= 1
+    assert np.array_equal(lg.dt, log_o.dt[1:])  # the first attempt ran through the host path
+    _assert_state_equal(s.download(), o.state(), "after rejections")
+
+
+def test_accepted_step_cap(pcl, oracle_lib):
+    c = ctl.dam_break_control(64, limiter=1, time_final=10.0)
+    cu = ctl.CustomSettings(max_accepted_steps=37)
+    s, o = _pair(c, cu)
+    q = ic.gaussian_bumps(64, 64, seed=3)
+    _start(s, o, q)
+    st = s.advance()
+    log_o = o.run()
+    assert st.accepted == log_o.accepted == 37
+    _assert_state_equal(s.download(), o.state(), "37 steps")
+
+
+@pytest.mark.parametrize("kind", ["nan", "negative"])
+def test_bad_state_is_reported(pcl, kind):
+    from paraclaws_b200._lib import PclError, PCL_ERR_NAN, PCL_ERR_NEG_DEPTH
+    c = ctl.dam_break_control(32)
+    s = Solver(c)
+    q = ic.circular_dam(32, 32)
+    q[10, 12, 0] = np.nan if kind == "nan" else -0.5
+    s.upload(q)
+    s.update_rank_boundaries()
+    with pytest.raises(PclError) as e:
+        s.advance()
+    assert e.value.code == (PCL_ERR_NAN if kind == "nan" else PCL_ERR_NEG_DEPTH)
