@@ -50,7 +50,7 @@ def needs_build() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    deps = [CSRC / s for s, _ in SOURCES] + HEADERS + [Path(__file__)]
+    deps = [CSRC / s for s, _ in SOURCES] + HEADERS + [Path(__file__), HOST_SRC]
     return any(p.stat().st_mtime > t for p in deps if p.exists())
 
 
@@ -75,7 +75,24 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
     os.replace(tmp, LIB)
+    build_host_driver()
     return LIB
+
+
+HOST_SRC = PKG / "host" / "paraclaws_main.cpp"
+HOST_BIN = PKG / "bin" / "paraclaws"
+
+
+def build_host_driver() -> Path:
+    """The C++ host program (main.f90 above the C ABI), linked against the in-tree library."""
+    HOST_BIN.parent.mkdir(exist_ok=True)
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", str(ROOT / "include"), str(HOST_SRC),
+           "-L", str(PKG), "-lparaclaws_b200", "-Wl,-rpath,$ORIGIN/..", "-o", str(HOST_BIN)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("host driver build failed")
+    return HOST_BIN
 
 
 if __name__ == "__main__":
