@@ -151,6 +151,31 @@ int pcl_profile_kernels(pcl_ctx* ctx, int reps, double* avg_ms, int* nkinds);
 /* Copy up to cap records of the device step log; *n = records logged so far. */
 int pcl_get_step_log(pcl_ctx* ctx, pcl_step_record* out, long long cap, long long* n);
 
+/* ---- one step without device allocation ---- */
+
+/* No counterpart in the reference.  One attempted FP64 step -- the xi and eta sweeps and the
+   accept/reject test of pcl_solve_dimensional_split, bit-identical to it -- for callers that
+   cannot allocate device memory: hosts whose device memory belongs to another allocator, step
+   loops that must not pay the device-wide synchronisation of cudaMalloc/cudaFree, or jobs that
+   must account for all device memory up front.  It allocates nothing: its scratch (the
+   intermediate state, mesh tables and control block) is one static device array in the library,
+   held by every GPU that loads the library (about 1.6 MB) until exit, which limits the grid to
+   m_xi, m_eta <= 128 (larger grids return PCL_ERR_BADARG).
+   - d_state_in / d_state_out: caller-owned device memory, three planes (h, hu, hv), each of
+     m_eta+4 rows of ld >= m_xi+4 doubles, plane p at base + p*ld*(m_eta+4), cell (i, j) of the
+     padded block (i, j = -1 .. m+2) at row j+1, column i+1.  The input's ghost cells must be
+     filled (pcl_update_rank_boundaries semantics).  The output gets the new interior plus the
+     input's ghost cells, and is written only when *ierr = 1.
+   - dt: the step size; ctl supplies the grid, limiter, boundary codes, grav, cfl_limit and
+     dt_min_shrink_ratio (precision_mode must be FP64).  *cfl receives the attempt's CFL.
+   - stream: a cudaStream_t or NULL; the call synchronises it before returning.
+   The first call on a device looks up the array's device address (once per device); make that
+   first call before any stream capture.  All calls share the array and it keeps the last
+   call's contents; calls that overlap on the GPU race on it. */
+int pcl_solve_dimensional_split_noalloc(const pcl_solver_control* ctl, int device, void* stream,
+                                        const double* d_state_in, double* d_state_out, long long ld,
+                                        double dt, double* cfl, int* ierr);
+
 /* ---- utilities ---- */
 int pcl_synchronize(pcl_ctx* ctx);
 void* pcl_get_stream(pcl_ctx* ctx);                   /* the context's cudaStream_t */

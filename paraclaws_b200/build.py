@@ -25,6 +25,7 @@ SOURCES = [
     ("kernels_aux.cu", False),
     ("kernels_mixed.cu", True),
     ("capi.cu", False),
+    ("noalloc.cu", False),
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

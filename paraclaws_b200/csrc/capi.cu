@@ -225,7 +225,7 @@ static int validate(const pcl_solver_control* c) {
 }
 
 // mesh tables in the reference's operation order (domain/SMOD_mesh_manipulation.f90)
-static void build_tables(const pcl_solver_control* c, double dxi, double deta, std::vector<double>& rowm,
+void build_tables(const pcl_solver_control* c, double dxi, double deta, std::vector<double>& rowm,
                          std::vector<double>& colm) {
   const int ni = c->m_xi + 4, nj = c->m_eta + 4;
   rowm.assign((size_t)nj * kRowMetrics, 0.0);
