@@ -151,6 +151,18 @@ int pcl_profile_kernels(pcl_ctx* ctx, int reps, double* avg_ms, int* nkinds);
 /* Copy up to cap records of the device step log; *n = records logged so far. */
 int pcl_get_step_log(pcl_ctx* ctx, pcl_step_record* out, long long cap, long long* n);
 
+/* ---- precision form support ---- */
+
+/* FP64 sums of h, hu and hv over the interior cells of the current solution (mass and
+   momentum; multiply by d_xi*d_eta for the integrals).  Rows are summed on the device and the
+   row partials added on the host in row order, so the result is reproducible.  No counterpart
+   in the reference (it has no conservation diagnostics). */
+int pcl_conservation_sums(pcl_ctx* ctx, double* sums3);
+
+/* Rows per work item of the fused mixed-precision kernel (default 64; the autotuner sets it).
+   No effect on results: every cell's arithmetic is independent of the tiling. */
+int pcl_set_tile_rows(pcl_ctx* ctx, int rows);
+
 /* ---- one step without device allocation ---- */
 
 /* No counterpart in the reference.  One attempted FP64 step -- the xi and eta sweeps and the

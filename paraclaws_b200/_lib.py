@@ -118,6 +118,8 @@ def load(build_if_missing: bool = True):
     L.pcl_device_bytes.argtypes = [vp]
     L.pcl_device_bytes.restype = C.c_longlong
     L.pcl_get_io_bytes.argtypes = [vp, P(C.c_longlong), P(C.c_longlong)]
+    L.pcl_conservation_sums.argtypes = [vp, P(C.c_double)]
+    L.pcl_set_tile_rows.argtypes = [vp, C.c_int]
     L.pcl_solve_dimensional_split_noalloc.argtypes = [P(SolverControl), C.c_int, vp, vp, vp, C.c_longlong,
                                                       C.c_double, P(C.c_double), P(C.c_int)]
     L.pcl_host_alloc.argtypes = [P(vp), C.c_longlong]

@@ -661,6 +661,36 @@ int pcl_get_step_log(pcl_ctx* x, pcl_step_record* out, long long cap, long long*
   return PCL_OK;
 }
 
+int pcl_conservation_sums(pcl_ctx* x, double* sums) {
+  if (!x || !sums) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  // the AoS staging buffer (3 doubles per padded cell) holds the 3 partials of each row
+  launch_row_sums(x->g, x->staging_d, x->stream);
+  x->launches += 1;
+  int r = check_launch(x);
+  if (r != PCL_OK) return r;
+  std::vector<double> part((size_t)3 * x->cfg.m_eta);
+  x->d2h_bytes += (long long)(sizeof(double) * part.size());
+  CK(cudaMemcpyAsync(part.data(), x->staging_d, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int j = 0; j < x->cfg.m_eta; ++j)
+    for (int p = 0; p < 3; ++p) s[p] += part[(size_t)j * 3 + p];
+  for (int p = 0; p < 3; ++p) sums[p] = s[p];
+  return PCL_OK;
+}
+
+int pcl_set_tile_rows(pcl_ctx* x, int rows) {
+  if (!x || rows < 4) return PCL_ERR_BADARG;
+  if (x->mixed) mixed_set_tile_rows(x->mixed, rows);
+  if (x->graph) {  // the captured launches carry the old tiling
+    cudaGraphExecDestroy(x->graph);
+    x->graph = nullptr;
+    x->graph_chunk = 0;
+  }
+  return PCL_OK;
+}
+
 int pcl_get_io_bytes(pcl_ctx* x, long long* h2d, long long* d2h) {
   if (!x) return PCL_ERR_BADARG;
   if (h2d) *h2d = x->h2d_bytes;

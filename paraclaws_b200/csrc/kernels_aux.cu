@@ -281,6 +281,33 @@ __global__ void download_kernel(GridDev g, double* __restrict__ aos) {
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// FP64 conservation sums over the interior: each block sums whole rows in a fixed order and
+// writes one partial per row; the host adds the partials in row order, so the result does not
+// depend on scheduling.
+// ------------------------------------------------------------------------------------------
+__global__ void row_sums_kernel(GridDev g, double* __restrict__ partial) {
+  __shared__ double red[3][256];
+  const int j = 1 + blockIdx.x;
+  const double* b = buffer(g, g.ctl->cur) + (long long)(j + 1) * g.pitch;
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int i = 1 + threadIdx.x; i <= g.mx; i += blockDim.x)
+    for (int p = 0; p < 3; ++p) s[p] += b[p * g.plane + i + 1];
+  for (int p = 0; p < 3; ++p) red[p][threadIdx.x] = s[p];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int p = 0; p < 3; ++p) red[p][threadIdx.x] += red[p][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int p = 0; p < 3; ++p) partial[(long long)blockIdx.x * 3 + p] = red[p][0];
+}
+
+void launch_row_sums(const GridDev& g, double* partial, cudaStream_t st) {
+  row_sums_kernel<<<g.my, 256, 0, st>>>(g, partial);
+}
+
 void launch_upload(const GridDev& g, const double* staging_aos, cudaStream_t st) {
   upload_kernel<<<148 * 8, 256, 0, st>>>(g, staging_aos);
 }

@@ -206,6 +206,14 @@ class Solver:
         _lib.check(self.L.pcl_get_io_bytes(self.h, C.byref(h2d), C.byref(d2h)), "pcl_get_io_bytes")
         return {"h2d": h2d.value, "d2h": d2h.value}
 
+    def conservation_sums(self) -> np.ndarray:
+        out = (C.c_double * 3)()
+        _lib.check(self.L.pcl_conservation_sums(self.h, out), "pcl_conservation_sums")
+        return np.array(list(out))
+
+    def set_tile_rows(self, rows: int) -> None:
+        _lib.check(self.L.pcl_set_tile_rows(self.h, int(rows)), "pcl_set_tile_rows")
+
     def reset_time_control(self) -> None:
         _lib.check(self.L.pcl_reset_time_control(self.h), "pcl_reset_time_control")
 
