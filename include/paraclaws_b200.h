@@ -151,6 +151,39 @@ int pcl_profile_kernels(pcl_ctx* ctx, int reps, double* avg_ms, int* nkinds);
 /* Copy up to cap records of the device step log; *n = records logged so far. */
 int pcl_get_step_log(pcl_ctx* ctx, pcl_step_record* out, long long cap, long long* n);
 
+/* ---- batching form ----
+   No counterpart in the reference (one run = one grid there).  Many independent grids of
+   uneven size ("instances"), each with its own control.in settings, state and adaptive dt
+   (its own time_control), advanced together by ONE persistent kernel launch per attempted step
+   (captured in CUDA graphs).  Each launch runs, for every instance that is not done, exactly
+   what pcl_advance runs for one attempt (sweeps, accept/reject, updateTime, snapshot index,
+   ghost fill), with bit-identical results.  Instances can be added and removed between steps. */
+typedef struct pcl_batch pcl_batch;
+
+/* precision: PCL_PREC_FP64 or PCL_PREC_MIXED (every instance of a batch uses it). */
+int pcl_batch_create(int device, int precision, int max_instances, pcl_batch** out);
+int pcl_batch_destroy(pcl_batch* batch);
+/* device bytes one instance with these settings holds (state buffers, tables, control, log) */
+long long pcl_batch_instance_bytes(const pcl_solver_control* ctl);
+/* Allocate a slot, upload the state (reference layout), fill its ghosts: *slot receives its id.
+   PCL_ERR_FULL when no slot is free. */
+int pcl_batch_add(pcl_batch* batch, const pcl_solver_control* ctl, const double* vars, int* slot);
+int pcl_batch_remove(pcl_batch* batch, int slot);
+/* nsteps attempted steps of every instance not done (persistent launches, graphs of 16). */
+int pcl_batch_step(pcl_batch* batch, int nsteps);
+/* done[slot] (1 done, 0 running, -1 free slot) and status[slot] (PCL_* code) of every slot;
+   arrays of max_instances entries. */
+int pcl_batch_poll(pcl_batch* batch, int* done, int* status);
+int pcl_batch_stats(pcl_batch* batch, int slot, pcl_run_stats* stats);
+int pcl_batch_download(pcl_batch* batch, int slot, double* vars);
+int pcl_batch_get_step_log(pcl_batch* batch, int slot, pcl_step_record* out, long long cap, long long* n);
+/* Schedule of the persistent kernel (set by the autotuner): rows per mixed work item, rows per
+   FP64 xi item, rows per FP64 eta strip, CTAs per SM (0: the occupancy limit).  Results do not
+   depend on it. */
+int pcl_batch_set_schedule(pcl_batch* batch, int tile_rows, int x_rows, int y_rows, int blocks_per_sm);
+int pcl_batch_info(pcl_batch* batch, int* n_used, int* n_done, long long* cells, long long* device_bytes);
+void* pcl_batch_get_stream(pcl_batch* batch);
+
 /* ---- precision form support ---- */
 
 /* FP64 sums of h, hu and hv over the interior cells of the current solution (mass and

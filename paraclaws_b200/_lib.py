@@ -119,6 +119,21 @@ def load(build_if_missing: bool = True):
     L.pcl_device_bytes.restype = C.c_longlong
     L.pcl_get_io_bytes.argtypes = [vp, P(C.c_longlong), P(C.c_longlong)]
     L.pcl_conservation_sums.argtypes = [vp, P(C.c_double)]
+    L.pcl_batch_create.argtypes = [C.c_int, C.c_int, C.c_int, P(vp)]
+    L.pcl_batch_destroy.argtypes = [vp]
+    L.pcl_batch_instance_bytes.argtypes = [P(SolverControl)]
+    L.pcl_batch_instance_bytes.restype = C.c_longlong
+    L.pcl_batch_add.argtypes = [vp, P(SolverControl), vp, P(C.c_int)]
+    L.pcl_batch_remove.argtypes = [vp, C.c_int]
+    L.pcl_batch_step.argtypes = [vp, C.c_int]
+    L.pcl_batch_poll.argtypes = [vp, P(C.c_int), P(C.c_int)]
+    L.pcl_batch_stats.argtypes = [vp, C.c_int, P(RunStats)]
+    L.pcl_batch_download.argtypes = [vp, C.c_int, vp]
+    L.pcl_batch_get_step_log.argtypes = [vp, C.c_int, P(StepRecord), C.c_longlong, P(C.c_longlong)]
+    L.pcl_batch_set_schedule.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.pcl_batch_info.argtypes = [vp, P(C.c_int), P(C.c_int), P(C.c_longlong), P(C.c_longlong)]
+    L.pcl_batch_get_stream.argtypes = [vp]
+    L.pcl_batch_get_stream.restype = vp
     L.pcl_set_tile_rows.argtypes = [vp, C.c_int]
     L.pcl_solve_dimensional_split_noalloc.argtypes = [P(SolverControl), C.c_int, vp, vp, vp, C.c_longlong,
                                                       C.c_double, P(C.c_double), P(C.c_int)]

@@ -1,0 +1,198 @@
+"""Batching form: many independent dam-break grids of uneven size advanced by one persistent
+kernel launch per attempted step (C ABI pcl_batch_*), and the project autotuner that picks the
+launch schedule.
+
+Every instance keeps its own control.in settings, state and adaptive dt.  Results are
+bit-identical to running each instance alone with ``Solver.advance``: the schedule decides
+which CTA runs which piece of work, never what a cell computes.  That also lets the autotuner
+time candidate schedules on real steps of the batch it tunes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import time
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .control import ControlSettings, CustomSettings, PRECISION_FP64, PRECISION_MIXED
+from .solver import Stats, StepLog, to_c_control
+
+
+@dataclass
+class Schedule:
+    tile_rows: int = 64     # rows per mixed work item
+    x_rows: int = 8         # rows per FP64 xi item
+    y_rows: int = 32        # rows per FP64 eta strip
+    blocks_per_sm: int = 0  # persistent CTAs per SM (0: occupancy limit)
+
+
+class Batch:
+    """A set of instances on one GPU stepped together (one precision per batch)."""
+
+    def __init__(self, max_instances: int, precision: int = PRECISION_FP64, device: int = 0):
+        self.L = _lib.load()
+        self.precision = int(precision)
+        self.max_instances = int(max_instances)
+        h = C.c_void_p()
+        _lib.check(self.L.pcl_batch_create(int(device), self.precision, self.max_instances, C.byref(h)),
+                   "pcl_batch_create")
+        self.h = h
+        self.shapes: Dict[int, Tuple[int, int, int]] = {}
+        self.schedule = Schedule()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.pcl_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def instance_bytes(control: ControlSettings, custom: Optional[CustomSettings] = None, precision=None) -> int:
+        L = _lib.load()
+        c = to_c_control(control, custom, precision)
+        return int(L.pcl_batch_instance_bytes(C.byref(c)))
+
+    def add(self, control: ControlSettings, q: np.ndarray, custom: Optional[CustomSettings] = None) -> int:
+        c = to_c_control(control, custom, self.precision)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        shape = (control.m_eta + 4, control.m_xi + 4, 3)
+        if q.shape != shape:
+            raise ValueError(f"state shape {q.shape} != {shape}")
+        slot = C.c_int()
+        _lib.check(self.L.pcl_batch_add(self.h, C.byref(c), q.ctypes.data, C.byref(slot)), "pcl_batch_add")
+        self.shapes[slot.value] = shape
+        return slot.value
+
+    def remove(self, slot: int) -> None:
+        _lib.check(self.L.pcl_batch_remove(self.h, int(slot)), "pcl_batch_remove")
+        self.shapes.pop(slot, None)
+
+    def step(self, nsteps: int = 1) -> None:
+        _lib.check(self.L.pcl_batch_step(self.h, int(nsteps)), "pcl_batch_step")
+
+    def poll(self) -> Tuple[np.ndarray, np.ndarray]:
+        done = (C.c_int * self.max_instances)()
+        status = (C.c_int * self.max_instances)()
+        _lib.check(self.L.pcl_batch_poll(self.h, done, status), "pcl_batch_poll")
+        return np.array(done[:], dtype=np.int32), np.array(status[:], dtype=np.int32)
+
+    def stats(self, slot: int) -> Stats:
+        s = _lib.RunStats()
+        _lib.check(self.L.pcl_batch_stats(self.h, int(slot), C.byref(s)), "pcl_batch_stats")
+        return Stats.from_c(s)
+
+    def download(self, slot: int) -> np.ndarray:
+        out = np.empty(self.shapes[slot], dtype=np.float64)
+        _lib.check(self.L.pcl_batch_download(self.h, int(slot), out.ctypes.data), "pcl_batch_download")
+        return out
+
+    def step_log(self, slot: int) -> StepLog:
+        n = C.c_longlong()
+        _lib.check(self.L.pcl_batch_get_step_log(self.h, int(slot), None, 0, C.byref(n)), "pcl_batch_get_step_log")
+        recs = (_lib.StepRecord * max(n.value, 1))()
+        _lib.check(self.L.pcl_batch_get_step_log(self.h, int(slot), recs, n.value, C.byref(n)),
+                   "pcl_batch_get_step_log")
+        arr = np.frombuffer(recs, dtype=np.dtype([("dt", "f8"), ("cfl", "f8"), ("time", "f8"), ("dt_next", "f8"),
+                                                  ("ierr", "i4"), ("snap", "i4")]), count=n.value)
+        return StepLog(arr["dt"].copy(), arr["cfl"].copy(), arr["time"].copy(), arr["dt_next"].copy(),
+                       arr["ierr"].copy(), arr["snap"].copy())
+
+    def set_schedule(self, s: Schedule) -> None:
+        _lib.check(self.L.pcl_batch_set_schedule(self.h, s.tile_rows, s.x_rows, s.y_rows, s.blocks_per_sm),
+                   "pcl_batch_set_schedule")
+        self.schedule = s
+
+    def info(self) -> dict:
+        used, done = C.c_int(), C.c_int()
+        cells, nbytes = C.c_longlong(), C.c_longlong()
+        _lib.check(self.L.pcl_batch_info(self.h, C.byref(used), C.byref(done), C.byref(cells), C.byref(nbytes)),
+                   "pcl_batch_info")
+        return {"used": used.value, "done": done.value, "cells": cells.value, "device_bytes": nbytes.value}
+
+    @property
+    def stream(self) -> int:
+        return self.L.pcl_batch_get_stream(self.h) or 0
+
+
+# ------------------------------------------------------------------------------------------
+# autotuner
+# ------------------------------------------------------------------------------------------
+def candidate_schedules(precision: int) -> List[Schedule]:
+    if precision == PRECISION_MIXED:
+        return [Schedule(tile_rows=tr, blocks_per_sm=b) for tr in (16, 32, 64, 128) for b in (0, 2, 3)]
+    return [Schedule(x_rows=xr, y_rows=yr, blocks_per_sm=b) for xr in (4, 8, 16) for yr in (16, 32, 64) for b in (0, 1)]
+
+
+def _signature(batch: Batch) -> str:
+    sides = sorted((s[1] - 4, s[0] - 4) for s in batch.shapes.values())
+    # coarse histogram of grid sizes: the schedule depends on the mix, not on each grid
+    hist = np.histogram([a * b for a, b in sides], bins=[0, 64 ** 2, 128 ** 2, 256 ** 2, 512 ** 2, 1024 ** 2,
+                                                          2048 ** 2, 1 << 40])[0]
+    return f"p{batch.precision}-n{len(sides)}-h{'.'.join(str(int(x)) for x in hist)}"
+
+
+def _device_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(0).replace(" ", "_")
+    except Exception:
+        return "cuda"
+
+
+def default_cache() -> Path:
+    base = Path(os.environ.get("XDG_CACHE_HOME", Path.home() / ".cache"))
+    return base / "paraclaws_b200" / "autotune.json"
+
+
+def autotune(batch: Batch, steps_per_trial: int = 8, candidates: Optional[Sequence[Schedule]] = None,
+             cache: Optional[Path] = None, use_cache: bool = True) -> Tuple[Schedule, Dict[str, float]]:
+    """Time each candidate schedule on real steps of `batch` (CUDA events on its stream) and set
+    the fastest.  The steps count as simulation progress: the schedule never changes results.
+    Results are cached per (GPU, precision, grid-size histogram)."""
+    import torch
+    cache = Path(cache) if cache else default_cache()
+    key = f"{_device_name()}:{_signature(batch)}"
+    table = {}
+    if use_cache and cache.exists():
+        try:
+            table = json.loads(cache.read_text())
+        except ValueError:
+            table = {}
+    if use_cache and key in table:
+        best = Schedule(**table[key]["schedule"])
+        batch.set_schedule(best)
+        return best, table[key]["ms_per_step"]
+    cands = list(candidates) if candidates else candidate_schedules(batch.precision)
+    stream = torch.cuda.ExternalStream(batch.stream)
+    timings: Dict[str, float] = {}
+    best, best_ms = None, float("inf")
+    for s in cands:
+        batch.set_schedule(s)
+        batch.step(2)  # rebuild items, warm up
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.step(steps_per_trial)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps_per_trial
+        timings[json.dumps(s.__dict__, sort_keys=True)] = ms
+        if ms < best_ms:
+            best, best_ms = s, ms
+    batch.set_schedule(best)
+    if use_cache:
+        table[key] = {"schedule": best.__dict__, "ms_per_step": timings}
+        cache.parent.mkdir(parents=True, exist_ok=True)
+        cache.write_text(json.dumps(table, indent=1))
+    return best, timings

@@ -1,7 +1,8 @@
 """Build libparaclaws_b200.so in-tree with nvcc for sm_100a.
 
-The FP64 parity translation units are compiled with --fmad=false (no contraction, so results
-round where the reference's source rounds); the mixed-precision unit keeps FMA contraction.
+Every translation unit is compiled with --fmad=false: the FP64 parity code must round where
+the reference's source rounds, and the mixed-precision code writes its multiply-adds out
+explicitly so its bits do not depend on the kernel it is inlined into.
 Host code is compiled with -ffp-contract=off for the same reason.
 """
 from __future__ import annotations
@@ -23,8 +24,11 @@ HEADERS = [ROOT / "include" / "paraclaws_b200.h"] + sorted(CSRC.glob("*.h")) + s
 SOURCES = [
     ("kernels_fp64.cu", False),
     ("kernels_aux.cu", False),
-    ("kernels_mixed.cu", True),
+    ("kernels_mixed.cu", False),
+    ("batch_fp64.cu", False),
+    ("batch_mixed.cu", False),
     ("capi.cu", False),
+    ("capi_batch.cu", False),
     ("noalloc.cu", False),
 ]
 

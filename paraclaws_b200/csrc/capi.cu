@@ -209,7 +209,7 @@ int pcl_read_solver_control(const char* control_in, const char* custom_in, pcl_s
   return PCL_OK;
 }
 
-static int validate(const pcl_solver_control* c) {
+int validate_control(const pcl_solver_control* c) {
   if (c->num_equations != 3 || c->num_waves != 2 || c->num_ghost != 2) return PCL_ERR_BADARG;
   if (c->m_xi < 2 || c->m_eta < 2) return PCL_ERR_BADARG;
   const int bcs[4] = {c->bc_xi_lower, c->bc_xi_upper, c->bc_eta_lower, c->bc_eta_upper};
@@ -251,7 +251,7 @@ void build_tables(const pcl_solver_control* c, double dxi, double deta, std::vec
 }
 
 // time_control%initialize (MOD_time_control.f90:70-151)
-static void init_ctl(const pcl_solver_control* c, Ctl& t) {
+void init_ctl(const pcl_solver_control* c, Ctl& t) {
   std::memset(&t, 0, sizeof(t));
   t.time_initial = c->t_start;
   t.time_final = c->t_final;
@@ -294,7 +294,7 @@ static void free_ctx(pcl_ctx* x) {
 int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
   if (!c || !out) return PCL_ERR_BADARG;
   *out = nullptr;
-  int v = validate(c);
+  int v = validate_control(c);
   if (v != PCL_OK) return v;
   CK(cudaSetDevice(device));
   pcl_ctx* x = new pcl_ctx();

@@ -1,0 +1,318 @@
+// pcl_sweeps_fp64.cuh -- the FP64 parity sweeps as device functions, shared by the per-sweep
+// kernels of a single grid (kernels_fp64.cu) and the persistent batched kernel
+// (batch_fp64.cu).  Include only from translation units built with --fmad=false.
+//
+// Buffer rotation replaces solution_old = solution (main.f90:201): the xi sweep reads buffer
+// cur and writes the interior rows of buffer (cur+1)%3; the eta sweep reads those rows plus the
+// pre-step ghost rows of buffer cur (ghosts are filled once per accepted step, main.f90:246) and
+// writes buffer (cur+2)%3.  A rejected attempt never touches buffer cur.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pcl_fp64.cuh"
+
+namespace pcl {
+
+
+// CFL bookkeeping shared by both sweeps: block max of s2, one atomic per block.
+template <int NT>
+__device__ __forceinline__ void block_max_to(unsigned long long* dst, double v, double* red) {
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double w = lane < NT / 32 ? red[lane] : 0.0;
+    w = warp_max(w);
+    if (lane == 0) atomic_max_nonneg(dst, w);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// xi sweep.  One CTA = one row segment of L = NT-4 cells.  Thread t owns cell i0-2+t (phase A),
+// interface i0-1+t (phase B), interface i0+t (phase C) and cell i0+t (phase D).
+// ------------------------------------------------------------------------------------------
+// Shared memory of one xi-sweep segment (per-slot cell data, waves, correction flux).
+template <int NT>
+struct XSmem {
+  double sq[3][NT], sf[3][NT], ss[NT], sk[NT];
+  double sw1[3][NT], sw2[3][NT], ss2[NT], sft[3][NT];
+  double red[NT / 32];
+};
+
+template <int NT, int LIM, bool SO>
+__device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S) {
+  const Ctl* ctl = g.ctl;
+  constexpr int L = NT - 4;
+  const int cur = ctl->cur, out = cur == 2 ? 0 : cur + 1;
+  const double dtod = ctl->dtod_x;
+  const int t = threadIdx.x;
+  const int mx = g.mx;
+  const long long row = (long long)(j + 1) * g.pitch;
+  const double* q0 = buffer(g, cur) + row;
+  const double* q1 = q0 + g.plane;
+  const double* q2 = q1 + g.plane;
+
+  auto& sq = S.sq;
+  auto& sf = S.sf;
+  auto& ss = S.ss;
+  auto& sk = S.sk;
+  auto& sw1 = S.sw1;
+  auto& sw2 = S.sw2;
+  auto& ss2 = S.ss2;
+  auto& sft = S.sft;
+  auto& red = S.red;
+
+  // phase A: per-cell flux J.q, wave-speed bound and capacity
+  int bad = 0;
+  {
+    const int c = i0 - 2 + t;
+    if (c <= mx + 2) {
+      const double h = q0[c + 1], hu = q1[c + 1], hv = q2[c + 1];
+      int cb = 0;
+      const CellFlux F = cell_flux<0>(h, hu, hv, g.grav, &cb);
+      if (c <= mx + 1) bad |= cb;  // getJakobi runs on cells -1 .. m_xi+1 in the xi sweep
+      sq[0][t] = h; sq[1][t] = hu; sq[2][t] = hv;
+      sf[0][t] = F.f0; sf[1][t] = F.f1; sf[2][t] = F.f2;
+      ss[t] = F.s;
+      sk[t] = capacity(g.rowm, g.colm, c, j, g.area_scale);
+    }
+  }
+  __syncthreads();
+
+  // phase B: HLL at interface k = i0-1+t between cells k-1 (slot t) and k (slot t+1)
+  double smax = 0.0;
+  if (t < NT - 1) {
+    const int k = i0 - 1 + t;
+    Waves W;
+    double s2 = 0.0;
+    if (k <= mx + 1) {
+      const double qL[3] = {sq[0][t], sq[1][t], sq[2][t]};
+      const double qR[3] = {sq[0][t + 1], sq[1][t + 1], sq[2][t + 1]};
+      const CellFlux FL = {sf[0][t], sf[1][t], sf[2][t], ss[t]};
+      const CellFlux FR = {sf[0][t + 1], sf[1][t + 1], sf[2][t + 1], ss[t + 1]};
+      s2 = hll(qL, FL, qR, FR, W);
+      smax = s2;
+    } else {
+#pragma unroll
+      for (int me = 0; me < 3; ++me) W.w1[me] = W.w2[me] = 0.0;
+    }
+#pragma unroll
+    for (int me = 0; me < 3; ++me) {
+      sw1[me][t] = W.w1[me];
+      sw2[me][t] = W.w2[me];
+    }
+    ss2[t] = s2;
+  }
+  block_max_to<NT>(const_cast<unsigned long long*>(&g.ctl->smax_x), smax, red);
+  if (bad) atomicOr(&g.ctl->status, bad);
+  __syncthreads();
+
+  // phase C: correction flux at interface k = i0+t (slot t+1); limited for 1 <= k <= m_xi,
+  // the wave at k = m_xi+1 stays unlimited (MOD_flux_correction.f90:54-75 vs :159)
+  if constexpr (SO) {
+    if (t < NT - 3) {
+      const int k = i0 + t;
+      double ft[3] = {0.0, 0.0, 0.0};
+      if (k <= mx + 1) {
+        const int s = t + 1;
+        const double s2 = ss2[s];
+        const double cf = corr_coef(s2, dtod, sk[t + 1], sk[t + 2]);
+        if (cf != 0.0) {
+          const double w1[3] = {sw1[0][s], sw1[1][s], sw1[2][s]};
+          const double w2[3] = {sw2[0][s], sw2[1][s], sw2[2][s]};
+          double a[3], b[3];
+          if (LIM != 0 && k <= mx) {
+            const double w1m[3] = {sw1[0][s - 1], sw1[1][s - 1], sw1[2][s - 1]};
+            const double w1p[3] = {sw1[0][s + 1], sw1[1][s + 1], sw1[2][s + 1]};
+            const double w2m[3] = {sw2[0][s - 1], sw2[1][s - 1], sw2[2][s - 1]};
+            const double w2p[3] = {sw2[0][s + 1], sw2[1][s + 1], sw2[2][s + 1]};
+            limit_wave<LIM>(w1m, w1, w1p, false, a);  // lambda_1 = -s2 <= 0
+            limit_wave<LIM>(w2m, w2, w2p, s2 > 0.0, b);
+          } else {
+#pragma unroll
+            for (int me = 0; me < 3; ++me) {
+              a[me] = w1[me];
+              b[me] = w2[me];
+            }
+          }
+#pragma unroll
+          for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
+        }
+      }
+#pragma unroll
+      for (int me = 0; me < 3; ++me) sft[me][t] = ft[me];
+    }
+    __syncthreads();
+  }
+
+  // phase D: update of cell i = i0+t (MOD_solve.f90:207-221 and :268-278)
+  if (t < L) {
+    const int i = i0 + t;
+    if (i <= mx) {
+      const int c = t + 2;
+      const double gam = __ldg(g.rowm + (j + 1) * kRowMetrics + 2);
+      const double dtk = dtod / sk[c];
+      const double sp = ss2[t + 1];       // A+ at interface i:   s2 * W2
+      const double sm = -ss2[t + 2];      // A- at interface i+1: s1 * W1
+      double* o0 = buffer(g, out) + row;
+#pragma unroll
+      for (int me = 0; me < 3; ++me) {
+        const double ap = sp * sw2[me][t + 1];
+        const double am = sm * sw1[me][t + 2];
+        double q = sq[me][c] - dtk * (gam * ap + gam * am);
+        if constexpr (SO) q = q - dtk * (sft[me][t + 1] - sft[me][t]);
+        o0[me * g.plane + i + 1] = q;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// eta sweep.  One thread = one column i, marching over a strip of rows [j0, j1] with a
+// register window of three interfaces.  Loads of consecutive threads are consecutive doubles.
+// ------------------------------------------------------------------------------------------
+struct YCell {
+  double q[3];
+  CellFlux F;
+  double kap;
+};
+
+template <int LIM, bool SO>
+__device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, const Waves& Wp, double s2,
+                                            bool limited, double dtod, double kl, double kr, double ft[3]) {
+  const double cf = corr_coef(s2, dtod, kl, kr);
+  if (cf == 0.0) {
+    ft[0] = ft[1] = ft[2] = 0.0;
+    return;
+  }
+  double a[3], b[3];
+  if (LIM != 0 && limited) {
+    limit_wave<LIM>(Wm.w1, W.w1, Wp.w1, false, a);
+    limit_wave<LIM>(Wm.w2, W.w2, Wp.w2, s2 > 0.0, b);
+  } else {
+#pragma unroll
+    for (int me = 0; me < 3; ++me) {
+      a[me] = W.w1[me];
+      b[me] = W.w2[me];
+    }
+  }
+#pragma unroll
+  for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
+}
+
+template <int LIM, bool SO>
+__device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
+  Ctl* ctl = g.ctl;
+  // xi-sweep validity (MOD_solve.f90:107-120), recomputed here from the reduction word
+  {
+    // written by atomics of other CTAs in a batched launch: read at L2, not a stale L1 line
+    const double sx = __longlong_as_double((long long)__ldcg(&ctl->smax_x));
+    const double cflx = sx * ctl->dt / g.dxi;
+    const double cfl = fmax(ctl->CFL, cflx);
+    if (!(ctl->CFL_target / cfl >= ctl->shrink)) return;
+  }
+  const int cur = ctl->cur;
+  const int xb = cur == 2 ? 0 : cur + 1;
+  const int yb = cur == 0 ? 2 : cur - 1;
+  const double dtod = ctl->dtod_y;
+  const int mx = g.mx, my = g.my;
+  const int i = col0 + threadIdx.x;
+  const bool active = i <= mx;
+  const int ic = active ? i : mx;  // inactive lanes shadow a valid column and store nothing
+  const int j1 = min(j0 + strip_rows - 1, my);
+  const long long P = g.pitch;
+  const double* pre = buffer(g, cur);
+  const double* xsw = buffer(g, xb);
+  double* outp = buffer(g, yb);
+  const double gam = __ldg(g.colm + (ic + 1) * kColMetrics + 2);
+  int bad = 0;
+  double smax = 0.0;
+
+  auto load = [&](int jj, YCell& c) {
+    const double* src = (jj >= 1 && jj <= my) ? xsw : pre;
+    const long long o = (long long)(jj + 1) * P + (ic + 1);
+    c.q[0] = src[o];
+    c.q[1] = src[o + g.plane];
+    c.q[2] = src[o + 2 * g.plane];
+    int cb = 0;
+    c.F = cell_flux<1>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
+    if (jj <= my + 1) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
+    c.kap = SO ? capacity(g.rowm, g.colm, ic, jj, g.area_scale) : 1.0;
+  };
+  auto iface = [&](int k, const YCell& L, const YCell& R, Waves& W) -> double {
+    if (k > my + 1) {
+#pragma unroll
+      for (int me = 0; me < 3; ++me) W.w1[me] = W.w2[me] = 0.0;
+      return 0.0;
+    }
+    const double s2 = hll(L.q, L.F, R.q, R.F, W);
+    smax = fmax(smax, s2);
+    return s2;
+  };
+
+  // prologue: cells j0-2 .. j0+1, interfaces j0-1 .. j0+1, correction flux at j0
+  YCell cA, cB, cC;  // cells jj, jj+1, jj+2 of the window
+  Waves W0, W1, W2;  // interfaces jj, jj+1, jj+2
+  double s0, s1, s2w;
+  double ft0[3] = {0.0, 0.0, 0.0}, ft1[3] = {0.0, 0.0, 0.0};
+  {
+    YCell cm2, cm1;
+    Waves Wm;
+    load(j0 - 2, cm2);
+    load(j0 - 1, cm1);
+    const double sm = iface(j0 - 1, cm2, cm1, Wm);
+    (void)sm;
+    load(j0, cA);
+    s0 = iface(j0, cm1, cA, W0);
+    load(j0 + 1, cB);
+    s1 = iface(j0 + 1, cA, cB, W1);
+    if constexpr (SO) y_corr_flux<LIM, SO>(Wm, W0, W1, s0, true, dtod, cm1.kap, cA.kap, ft0);
+  }
+  for (int jj = j0; jj <= j1; ++jj) {
+    load(jj + 2, cC);
+    s2w = iface(jj + 2, cB, cC, W2);
+    if constexpr (SO) y_corr_flux<LIM, SO>(W0, W1, W2, s1, jj + 1 <= my, dtod, cA.kap, cB.kap, ft1);
+    const double kap = SO ? cA.kap : capacity(g.rowm, g.colm, ic, jj, g.area_scale);
+    const double dtk = dtod / kap;
+    const long long o = (long long)(jj + 1) * P + (ic + 1);
+#pragma unroll
+    for (int me = 0; me < 3; ++me) {
+      const double ap = s0 * W0.w2[me];
+      const double am = (-s1) * W1.w1[me];
+      double q = cA.q[me] - dtk * (gam * ap + gam * am);
+      if constexpr (SO) q = q - dtk * (ft1[me] - ft0[me]);
+      if (active) outp[o + me * g.plane] = q;
+    }
+    // slide the window
+    cA = cB;
+    cB = cC;
+    W0 = W1;
+    W1 = W2;
+    s0 = s1;
+    s1 = s2w;
+#pragma unroll
+    for (int me = 0; me < 3; ++me) ft0[me] = ft1[me];
+  }
+  // Carry the pre-step ghost cells into the new buffer: until update_rank_boundaries runs, the
+  // reference's solution keeps the ghosts of the previous fill (main.f90:210 vs :246).
+  if (active) {
+    auto copy_cell = [&](int ci, int cj) {
+      const long long o = (long long)(cj + 1) * P + (ci + 1);
+#pragma unroll
+      for (int me = 0; me < 3; ++me) outp[o + me * g.plane] = pre[o + me * g.plane];
+    };
+    if (j0 == 1) copy_cell(i, -1), copy_cell(i, 0);
+    if (j1 == my) copy_cell(i, my + 1), copy_cell(i, my + 2);
+    if (i == 1)
+      for (int jj = j0; jj <= j1; ++jj) copy_cell(-1, jj), copy_cell(0, jj);
+    if (i == mx)
+      for (int jj = j0; jj <= j1; ++jj) copy_cell(mx + 1, jj), copy_cell(mx + 2, jj);
+  }
+  if (!active) smax = 0.0, bad = 0;
+  smax = warp_max(smax);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ctl->smax_y, smax);
+  if (bad) atomicOr(&ctl->status, bad);
+}
+
+}  // namespace pcl

@@ -1,0 +1,124 @@
+"""Batching form: one persistent launch per step advances many grids of uneven size, each with
+its own dt.  Every instance must be bit-identical to the same grid advanced alone
+(Solver.advance), for both precisions, whatever the schedule and whoever else is in the batch."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from paraclaws_b200 import control as ctl
+from paraclaws_b200 import ic
+from paraclaws_b200.batch import Batch, Schedule, autotune
+from paraclaws_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances(n, seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        mx = int(rng.choice([20, 37, 64, 100, 131, 256, 300]))
+        my = int(rng.choice([16, 33, 64, 97, 128, 260]))
+        lim = int(rng.integers(1, 5))
+        bc = int(rng.integers(1, 4))
+        c = dataclasses.replace(ctl.dam_break_control(mx, limiter=lim, bc=bc, time_final=float(rng.uniform(0.01, 0.05))),
+                                m_eta=my, initial_timestep=float(rng.choice([1e-10, 1e-4, 2e-3])))
+        p = ic.seeded_dam_params(k, offset=0.25)
+        q = ic.circular_dam(mx, my, p.radius, p.h_in, p.h_out, p.x0, p.y0)
+        out.append((c, q))
+    return out
+
+
+def _alone(c, q, precision):
+    s = Solver(c, precision=precision)
+    s.upload(q)
+    s.update_rank_boundaries()
+    s.advance()
+    r = s.download(), s.step_log()
+    s.close()
+    return r
+
+
+@pytest.mark.parametrize("precision", [ctl.PRECISION_FP64, ctl.PRECISION_MIXED])
+def test_batch_equals_alone(pcl, precision):
+    inst = _instances(12, seed=precision)
+    b = Batch(16, precision=precision)
+    slots = [b.add(c, q) for c, q in inst]
+    for _ in range(400):
+        b.step(16)
+        done, status = b.poll()
+        assert np.all(status[slots] == 0)
+        if np.all(done[slots] == 1):
+            break
+    for s, (c, q) in zip(slots, inst):
+        qa, la = _alone(c, q, precision)
+        lb = b.step_log(s)
+        assert np.array_equal(lb.dt, la.dt)
+        assert np.array_equal(lb.ierr, la.ierr)
+        assert np.array_equal(b.download(s), qa)
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [ctl.PRECISION_FP64, ctl.PRECISION_MIXED])
+def test_schedule_does_not_change_results(pcl, precision):
+    inst = _instances(5, seed=7)
+    results = []
+    scheds = ([Schedule(tile_rows=16), Schedule(tile_rows=128, blocks_per_sm=1)] if precision == ctl.PRECISION_MIXED
+              else [Schedule(x_rows=4, y_rows=16), Schedule(x_rows=16, y_rows=64, blocks_per_sm=1)])
+    for sch in scheds:
+        b = Batch(8, precision=precision)
+        b.set_schedule(sch)
+        slots = [b.add(c, q) for c, q in inst]
+        b.step(40)
+        results.append([b.download(s) for s in slots])
+        b.close()
+    for a, c in zip(results[0], results[1]):
+        assert np.array_equal(a, c)
+
+
+def test_add_and_remove_between_steps(pcl):
+    """Membership changes between steps: a new instance starts from its own initial state and
+    ends bit-identical to running alone, even though it joined mid-flight."""
+    inst = _instances(4, seed=3)
+    b = Batch(4, precision=ctl.PRECISION_MIXED)
+    s0 = b.add(*inst[0])
+    s1 = b.add(*inst[1])
+    b.step(10)
+    b.remove(s1)
+    s2 = b.add(*inst[2])
+    s3 = b.add(*inst[3])
+    for _ in range(200):
+        b.step(16)
+        done, _ = b.poll()
+        if all(done[s] == 1 for s in (s0, s2, s3)):
+            break
+    for s, k in ((s0, 0), (s2, 2), (s3, 3)):
+        qa, _ = _alone(*inst[k], ctl.PRECISION_MIXED)
+        assert np.array_equal(b.download(s), qa)
+    b.close()
+
+
+def test_full_batch_is_reported(pcl):
+    from paraclaws_b200._lib import PclError, PCL_ERR_FULL
+    c, q = _instances(1)[0]
+    b = Batch(1)
+    b.add(c, q)
+    with pytest.raises(PclError) as e:
+        b.add(c, q)
+    assert e.value.code == PCL_ERR_FULL
+    b.close()
+
+
+def test_autotuner_picks_a_schedule(pcl, tmp_path):
+    inst = _instances(6, seed=11)
+    b = Batch(8, precision=ctl.PRECISION_MIXED)
+    for c, q in inst:
+        c.time_final = 100.0
+        b.add(c, q)
+    best, timings = autotune(b, steps_per_trial=4, cache=tmp_path / "t.json")
+    assert best in [Schedule(**__import__("json").loads(k)) for k in timings]
+    assert (tmp_path / "t.json").exists()
+    best2, _ = autotune(b, cache=tmp_path / "t.json")
+    assert best2 == best
+    b.close()
