@@ -101,6 +101,12 @@ int pcl_destroy(pcl_ctx* ctx);
 int pcl_upload_state(pcl_ctx* ctx, const double* vars);
 int pcl_download_state(pcl_ctx* ctx, double* vars);
 
+/* set_initial_conditions of the dam-break example on the device
+   (examples/2D_dam_break/cartesian/SMOD_set_initial_conditions.f90:34-46): h = dam_h_in where
+   sqrt(x^2 + y^2) < dam_radius at the cell centre (shifted by dam_x0, dam_y0), else dam_h_out,
+   hu = hv = 0, on the whole padded block.  Needs initial_condition = 1. */
+int pcl_initial_condition(pcl_ctx* ctx);
+
 /* ---- the hot path, one call per reference routine ---- */
 
 /* update_rank_boundaries (user_subroutines/SMOD_boundary_conditions.f90:17-56): on-device
@@ -165,8 +171,9 @@ int pcl_batch_create(int device, int precision, int max_instances, pcl_batch** o
 int pcl_batch_destroy(pcl_batch* batch);
 /* device bytes one instance with these settings holds (state buffers, tables, control, log) */
 long long pcl_batch_instance_bytes(const pcl_solver_control* ctl);
-/* Allocate a slot, upload the state (reference layout), fill its ghosts: *slot receives its id.
-   PCL_ERR_FULL when no slot is free. */
+/* Allocate a slot, upload the state (reference layout) -- or, with vars = NULL and
+   initial_condition = 1, build the dam-break state on the device -- and fill its ghosts: *slot
+   receives its id.  PCL_ERR_FULL when no slot is free. */
 int pcl_batch_add(pcl_batch* batch, const pcl_solver_control* ctl, const double* vars, int* slot);
 int pcl_batch_remove(pcl_batch* batch, int slot);
 /* nsteps attempted steps of every instance not done (persistent launches, graphs of 16). */

@@ -96,7 +96,7 @@ def load(build_if_missing: bool = True):
     L.pcl_destroy.argtypes = [vp]
     for name in ("pcl_upload_state", "pcl_download_state"):
         getattr(L, name).argtypes = [vp, vp]
-    for name in ("pcl_update_rank_boundaries", "pcl_restore_solution", "pcl_integrate_source_term",
+    for name in ("pcl_update_rank_boundaries", "pcl_restore_solution", "pcl_integrate_source_term", "pcl_initial_condition",
                  "pcl_reset_cfl", "pcl_advance_snapshot_index", "pcl_synchronize"):
         getattr(L, name).argtypes = [vp]
     L.pcl_solve_dimensional_split.argtypes = [vp, P(C.c_int)]

@@ -63,14 +63,19 @@ class Batch:
         c = to_c_control(control, custom, precision)
         return int(L.pcl_batch_instance_bytes(C.byref(c)))
 
-    def add(self, control: ControlSettings, q: np.ndarray, custom: Optional[CustomSettings] = None) -> int:
+    def add(self, control: ControlSettings, q: Optional[np.ndarray], custom: Optional[CustomSettings] = None) -> int:
+        """Add an instance with state `q` (reference layout), or with q = None the dam-break state
+        of `custom` built on the device."""
         c = to_c_control(control, custom, self.precision)
-        q = np.ascontiguousarray(q, dtype=np.float64)
         shape = (control.m_eta + 4, control.m_xi + 4, 3)
-        if q.shape != shape:
-            raise ValueError(f"state shape {q.shape} != {shape}")
+        ptr = None
+        if q is not None:
+            q = np.ascontiguousarray(q, dtype=np.float64)
+            if q.shape != shape:
+                raise ValueError(f"state shape {q.shape} != {shape}")
+            ptr = q.ctypes.data
         slot = C.c_int()
-        _lib.check(self.L.pcl_batch_add(self.h, C.byref(c), q.ctypes.data, C.byref(slot)), "pcl_batch_add")
+        _lib.check(self.L.pcl_batch_add(self.h, C.byref(c), ptr, C.byref(slot)), "pcl_batch_add")
         self.shapes[slot.value] = shape
         return slot.value
 

@@ -410,6 +410,19 @@ int pcl_upload_state(pcl_ctx* x, const double* vars) {
   return PCL_OK;
 }
 
+int pcl_initial_condition(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  if (x->cfg.initial_condition != 1) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  const pcl_solver_control& c = x->cfg;
+  launch_dam_ic(x->g, c.dam_radius, c.dam_h_in, c.dam_h_out, c.dam_x0, c.dam_y0, x->stream);
+  x->launches += 1;
+  int r = check_launch(x);
+  if (r != PCL_OK) return r;
+  CK(cudaStreamSynchronize(x->stream));
+  return PCL_OK;
+}
+
 int pcl_download_state(pcl_ctx* x, double* vars) {
   if (!x || !vars) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));

@@ -257,7 +257,8 @@ int pcl_batch_destroy(pcl_batch* b) {
 }
 
 int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars, int* slot_out) {
-  if (!b || !c || !vars || !slot_out) return PCL_ERR_BADARG;
+  if (!b || !c || !slot_out) return PCL_ERR_BADARG;
+  if (!vars && c->initial_condition != 1) return PCL_ERR_BADARG;
   int v = validate_control(c);
   if (v != PCL_OK) return v;
   if (c->precision_mode != b->precision) return PCL_ERR_BADARG;
@@ -302,7 +303,7 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   g.area_scale = dxi * deta;
   g.grav = c->grav;
   const size_t stg = sizeof(double) * 3 * (size_t)(c->m_xi + 4) * (c->m_eta + 4);
-  if (stg > b->staging_bytes) {
+  if (vars && stg > b->staging_bytes) {
     cudaFree(b->staging_d);
     b->staging_d = nullptr;
     if (cudaMalloc(&b->staging_d, stg) != cudaSuccess) {
@@ -317,8 +318,12 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   BCK(cudaMemcpyAsync(const_cast<double*>(g.colm), colm.data(), sizeof(double) * colm.size(), cudaMemcpyHostToDevice,
                       b->stream));
   BCK(cudaMemcpyAsync(g.ctl, h, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
-  BCK(cudaMemcpyAsync(b->staging_d, vars, stg, cudaMemcpyHostToDevice, b->stream));
-  launch_upload(g, b->staging_d, b->stream);
+  if (vars) {
+    BCK(cudaMemcpyAsync(b->staging_d, vars, stg, cudaMemcpyHostToDevice, b->stream));
+    launch_upload(g, b->staging_d, b->stream);
+  } else {
+    launch_dam_ic(g, c->dam_radius, c->dam_h_in, c->dam_h_out, c->dam_x0, c->dam_y0, b->stream);
+  }
   launch_ghost(g, 1, b->stream);
   launch_timectl(g, kOpInit, 0, 0.0, b->stream);
   b->launches += 3;
@@ -415,6 +420,13 @@ int pcl_batch_download(pcl_batch* b, int s, double* vars) {
   BCK(cudaSetDevice(b->device));
   const auto& c = b->slots[s].cfg;
   const size_t stg = sizeof(double) * 3 * (size_t)(c.m_xi + 4) * (c.m_eta + 4);
+  if (stg > b->staging_bytes) {
+    cudaFree(b->staging_d);
+    b->staging_d = nullptr;
+    b->staging_bytes = 0;
+    if (cudaMalloc(&b->staging_d, stg) != cudaSuccess) return PCL_ERR_OOM;
+    b->staging_bytes = stg;
+  }
   launch_download(b->slots[s].g, b->staging_d, b->stream);
   b->launches += 1;
   BCK(cudaMemcpyAsync(vars, b->staging_d, stg, cudaMemcpyDeviceToHost, b->stream));

@@ -103,6 +103,36 @@ __global__ void download_kernel(GridDev g, double* __restrict__ aos) {
 }
 
 // ------------------------------------------------------------------------------------------
+// set_initial_conditions of the dam-break example on the device
+// (examples/2D_dam_break/cartesian/SMOD_set_initial_conditions.f90:34-46): h = h_in where
+// sqrt(x^2 + y^2) < radius at the cell centre (shifted by x0, y0 when they are non-zero), else
+// h_out; hu = hv = 0; the padded block including ghosts, into every rotation buffer.  The cell
+// centres come from the mesh tables, so the bits equal the host generator's.
+// ------------------------------------------------------------------------------------------
+__global__ void dam_ic_kernel(GridDev g, double radius, double h_in, double h_out, double x0, double y0) {
+  const int ni = g.mx + 4, nj = g.my + 4;
+  const long long n = (long long)ni * nj;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int jj = (int)(c / ni), ii = (int)(c - (long long)jj * ni);
+    double x = __ldg(g.colm + ii * kColMetrics + 3);
+    double y = __ldg(g.rowm + jj * kRowMetrics + 3);
+    if (x0 != 0.0) x = x - x0;
+    if (y0 != 0.0) y = y - y0;
+    const double h = sqrt(x * x + y * y) < radius ? h_in : h_out;
+    const long long o = (long long)jj * g.pitch + ii;
+    for (int b = 0; b < 3; ++b) {
+      buffer(g, b)[o] = h;
+      buffer(g, b)[o + g.plane] = 0.0;
+      buffer(g, b)[o + 2 * g.plane] = 0.0;
+    }
+  }
+}
+
+void launch_dam_ic(const GridDev& g, double radius, double h_in, double h_out, double x0, double y0, cudaStream_t st) {
+  dam_ic_kernel<<<148 * 8, 256, 0, st>>>(g, radius, h_in, h_out, x0, y0);
+}
+
+// ------------------------------------------------------------------------------------------
 // FP64 conservation sums over the interior: each block sums whole rows in a fixed order and
 // writes one partial per row; the host adds the partials in row order, so the result does not
 // depend on scheduling.

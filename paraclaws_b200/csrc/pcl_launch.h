@@ -23,6 +23,8 @@ void launch_ysweep_fp64(const GridDev& g, cudaStream_t st);
 void launch_timectl(const GridDev& g, int op, int arg, double value, cudaStream_t st);
 void launch_ghost(const GridDev& g, int force, cudaStream_t st);
 void launch_upload(const GridDev& g, const double* staging_aos, cudaStream_t st);
+void launch_dam_ic(const GridDev& g, double radius, double h_in, double h_out, double x0, double y0,
+                   cudaStream_t st);
 void launch_row_sums(const GridDev& g, double* partial /* 3 per interior row */, cudaStream_t st);
 void launch_download(const GridDev& g, double* staging_aos, cudaStream_t st);
 

@@ -131,6 +131,10 @@ class Solver:
         _lib.check(self.L.pcl_download_state(self.h, out.ctypes.data), "pcl_download_state")
         return out
 
+    def initial_condition(self) -> None:
+        """The dam-break state of the custom settings, built on the device."""
+        _lib.check(self.L.pcl_initial_condition(self.h), "pcl_initial_condition")
+
     # -- reference routine boundary --
     def update_rank_boundaries(self) -> None:
         _lib.check(self.L.pcl_update_rank_boundaries(self.h), "pcl_update_rank_boundaries")
