@@ -223,6 +223,170 @@ def config_dict(args) -> dict:
             "parallelism": "replicas" if args.gpus > 1 else "single"}
 
 
+
+# ------------------------------------------------------------------------------------------
+# the other forms of the step, reported beside the plain FP64 line
+# ------------------------------------------------------------------------------------------
+def _timed_advance(s, steps, torch):
+    stream = torch.cuda.ExternalStream(s.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    st = s.advance(max_attempts=steps)
+    e1.record(stream)
+    e1.synchronize()
+    return st, e0.elapsed_time(e1)
+
+
+def form_mixed(m, steps, warmup, device, fp64_value):
+    """The precision form on the same workload (same initial state, same step count)."""
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200 import ic
+    from paraclaws_b200.solver import Solver
+    c = workload(m)
+    q = ic.gaussian_bumps(m, m, seed=0)
+    s = Solver(c, ctl.CustomSettings(max_accepted_steps=steps), device=device, precision=ctl.PRECISION_MIXED)
+    s.upload(q)
+    s.update_rank_boundaries()
+    s.advance(max_attempts=warmup)
+    s.upload(q)
+    s.update_rank_boundaries()
+    s.reset_time_control()
+    st, ms = _timed_advance(s, steps, torch)
+    value = st.accepted * m * m / (ms * 1e-3)
+    peak, _ = hbm_peak()
+    s.close()
+    return {"value": value, "unit": UNIT, "speedup_vs_fp64": value / fp64_value,
+            "effective_roofline_frac": value * BYTES_PER_CELL_UPDATE / 1e9 / peak,
+            "note": "fused xi+eta kernel: 48 B of HBM traffic per cell-update; the fraction is scored "
+                    "against the 96 B/cell-update roofline of the two-sweep step (effective)",
+            "ms_per_step": ms / max(steps, 1)}
+
+
+def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 300, 400, 500, 700, 1000)):
+    """Precision-form accuracy on the 8192^2 seeded dam break, 1000 accepted steps: the mixed
+    form against FP64 at checkpoints, beside the conditioning floor of the step itself -- FP64
+    against FP64 started from the same state with h raised by one ulp in 1% of the cells.  The
+    reference's flux J(q).q carries the pressure term g*h^2 (twice the shallow-water g*h^2/2),
+    so its characteristic speeds are u +- sqrt(2 g h) while HLL and the CFL condition use
+    u +- sqrt(g h); at CFL 0.9 the step amplifies rounding-level differences until they are
+    O(1e-2) after ~1000 steps, whatever arithmetic makes them."""
+    import numpy as np
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200 import ic
+    from paraclaws_b200.solver import Solver
+    p = ic.seeded_dam_params(seed)
+    c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=1.0e9)
+    cu = ctl.CustomSettings(max_accepted_steps=steps, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out)
+    q = ic.circular_dam(m, m, p.radius, p.h_in, p.h_out, 0.0, 0.0)
+    qp = q.copy()
+    rng = np.random.Generator(np.random.PCG64(7))
+    mask = rng.random(q.shape[:2]) < 0.01
+    qp[..., 0] = np.where(mask, np.nextafter(q[..., 0], np.inf), q[..., 0])
+    runs = {"fp64": (ctl.PRECISION_FP64, q), "mixed": (ctl.PRECISION_MIXED, q), "fp64_perturbed": (ctl.PRECISION_FP64, qp)}
+    solvers = {}
+    sums0 = {}
+    for name, (prec, q0) in runs.items():
+        s = Solver(c, cu, device=device, precision=prec)
+        s.upload(q0)
+        s.update_rank_boundaries()
+        sums0[name] = s.conservation_sums()
+        solvers[name] = s
+    del qp
+    ms = {k: 0.0 for k in runs}
+    done = 0
+    curve = []
+    names = ("h", "hu", "hv")
+    for cp in checkpoints:
+        for name, s in solvers.items():
+            st, t_ms = _timed_advance(s, cp - done, torch)
+            ms[name] += t_ms
+        done = cp
+        ref = solvers["fp64"].download()[2:-2, 2:-2]
+        scale = float(np.abs(ref[..., 0]).sum())
+        row = {"step": cp, "time": solvers["fp64"].stats().time}
+        for name in ("mixed", "fp64_perturbed"):
+            x = solvers[name].download()[2:-2, 2:-2]
+            row[name] = {"l1_rel": {names[k]: float(np.abs(x[..., k] - ref[..., k]).sum() / scale) for k in range(3)},
+                         "linf": {names[k]: float(np.abs(x[..., k] - ref[..., k]).max()) for k in range(3)}}
+            del x
+        curve.append(row)
+        del ref
+    out = {}
+    for name, s in solvers.items():
+        st = s.stats()
+        m1 = s.conservation_sums()
+        out[name] = {"value": st.accepted * m * m / (ms[name] * 1e-3), "ms": ms[name], "time": st.time,
+                     "accepted": st.accepted, "rejected": st.rejected,
+                     "mass_drift_rel": float((m1[0] - sums0[name][0]) / sums0[name][0])}
+        s.close()
+    last = curve[-1]
+    out["l1_rel"] = last["mixed"]["l1_rel"]
+    out["linf"] = last["mixed"]["linf"]
+    out["conditioning_floor_l1_rel"] = last["fp64_perturbed"]["l1_rel"]
+    out["curve"] = curve
+    out["workload"] = (f"{m}^2 seeded dam break (seed {seed}: radius {p.radius:.3f}, h_in/h_out {p.h_in:.3f}), "
+                       f"minmod, CFL 0.9, {steps} accepted steps")
+    out["note"] = ("L1 of each component relative to sum|h| of the FP64 result, Linf absolute; "
+                   "fp64_perturbed = FP64 from the same state with h raised by 1 ulp in 1% of the cells "
+                   "(the step's own amplification of rounding-level differences)")
+    return out
+
+
+def form_batch(device, n=512, steps=32):
+    """512 dam-break instances, sides log-uniform 64..1024 (multiples of 32), own dt each."""
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200 import ic
+    from paraclaws_b200.batch import Batch, autotune
+    sides = ic.log_uniform_sides(n, 64, 1024, 32, seed=2)
+    res = {}
+    for name, prec in (("fp64", ctl.PRECISION_FP64), ("mixed", ctl.PRECISION_MIXED)):
+        b = Batch(n, precision=prec, device=device)
+        for k, m in enumerate(sides):
+            p = ic.seeded_dam_params(k, offset=0.25)
+            cu = ctl.CustomSettings(precision_mode=prec, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out,
+                                    dam_x0=p.x0, dam_y0=p.y0)
+            b.add(ctl.dam_break_control(m, limiter=1, time_final=1.0e9), None, cu)
+        best, _ = autotune(b, steps_per_trial=4, use_cache=False)
+        stream = torch.cuda.ExternalStream(b.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        cells = sum(m * m for m in sides)
+        peak, _ = hbm_peak()
+        v = cells / (ms * 1e-3)
+        res[name] = {"value": v, "unit": UNIT, "ms_per_step": ms, "schedule": best.__dict__,
+                     "effective_roofline_frac": v * BYTES_PER_CELL_UPDATE / 1e9 / peak}
+        b.close()
+    res["instances"] = n
+    res["cells"] = sum(m * m for m in sides)
+    res["launches_per_step"] = 1
+    return res
+
+
+def form_serving(device):
+    """Poisson arrivals, sides log-uniform 128..2048, end time U(0.1, 1), 120 GB budget."""
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200.serve import SolveServer, poisson_requests
+    res = {}
+    for name, prec, n, rate in (("mixed", ctl.PRECISION_MIXED, 80, 12.0), ("fp64", ctl.PRECISION_FP64, 30, 3.0)):
+        reqs = poisson_requests(n, rate=rate, seed=3, precision=prec)
+        srv = SolveServer(precision=prec, budget_bytes=120e9, max_slots=512, steps_per_tick=16, device=device)
+        rep = srv.run(reqs, max_wall=240.0)
+        srv.close()
+        res[name] = {"rate_per_s": rate, **rep.summary()}
+    return res
+
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
@@ -355,6 +519,11 @@ def run_ours(args) -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(m)
+    if rank == 0 and world == 1 and not args.no_forms:
+        line["forms"] = {"mixed": form_mixed(m, args.steps, args.warmup, local, value),
+                         "batch": form_batch(local),
+                         "serving": form_serving(local),
+                         "precision": form_precision(local)}
     s.close()
     if dist is not None:
         dist.barrier()
@@ -372,6 +541,7 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the mixed/batch/serving/precision forms")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

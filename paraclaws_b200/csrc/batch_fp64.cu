@@ -19,30 +19,37 @@ namespace {
 
 constexpr int kThreads = 256;
 
-template <int LIM, bool SO>
+template <int LIM, bool SO, bool UM>
 __device__ __forceinline__ void run_item(const GridDev& g, int kind, int a, int b, const BatchView& v,
                                          XSmem<kThreads>& S) {
   if (kind == kItemX) {
     const int jend = min(a + v.x_rows - 1, g.my);
     for (int j = a; j <= jend; ++j) {
-      xsweep_segment<kThreads, LIM, SO>(g, j, b, S);
+      xsweep_segment<kThreads, LIM, SO, UM>(g, j, b, S);
       __syncthreads();  // the segment's shared arrays are reused by the next row
     }
   } else {
-    ysweep_strip<LIM, SO>(g, a, b, v.y_rows);
+    ysweep_strip<LIM, SO, UM>(g, a, b, v.y_rows);
+  }
+}
+
+template <bool UM>
+__device__ __forceinline__ void dispatch_lim(const GridDev& g, int kind, int a, int b, const BatchView& v,
+                                             XSmem<kThreads>& S) {
+  if (!g.second_order) return run_item<0, false, UM>(g, kind, a, b, v, S);
+  switch (g.limiter) {
+    case 1: return run_item<1, true, UM>(g, kind, a, b, v, S);
+    case 2: return run_item<2, true, UM>(g, kind, a, b, v, S);
+    case 3: return run_item<3, true, UM>(g, kind, a, b, v, S);
+    case 4: return run_item<4, true, UM>(g, kind, a, b, v, S);
+    default: return run_item<0, true, UM>(g, kind, a, b, v, S);
   }
 }
 
 __device__ __forceinline__ void dispatch_item(const GridDev& g, int kind, int a, int b, const BatchView& v,
                                               XSmem<kThreads>& S) {
-  if (!g.second_order) return run_item<0, false>(g, kind, a, b, v, S);
-  switch (g.limiter) {
-    case 1: return run_item<1, true>(g, kind, a, b, v, S);
-    case 2: return run_item<2, true>(g, kind, a, b, v, S);
-    case 3: return run_item<3, true>(g, kind, a, b, v, S);
-    case 4: return run_item<4, true>(g, kind, a, b, v, S);
-    default: return run_item<0, true>(g, kind, a, b, v, S);
-  }
+  if (g.unit_metric) return dispatch_lim<true>(g, kind, a, b, v, S);
+  return dispatch_lim<false>(g, kind, a, b, v, S);
 }
 
 __global__ void __launch_bounds__(kThreads, 2) batch_fp64_kernel(BatchView v) {

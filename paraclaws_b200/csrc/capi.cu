@@ -351,6 +351,11 @@ int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
   g.deta = deta;
   g.area_scale = dxi * deta;  // d_xi*d_eta (SMOD_mesh_manipulation.f90:173)
   g.grav = c->grav;
+  launch_metric_check(g, x->stream);
+  if (cudaMemcpyAsync(&x->ctl_h->nonunit_metric, &g.ctl->nonunit_metric, sizeof(int), cudaMemcpyDeviceToHost,
+                      x->stream) != cudaSuccess || cudaStreamSynchronize(x->stream) != cudaSuccess)
+    return fail(PCL_ERR_CUDA);
+  g.unit_metric = x->ctl_h->nonunit_metric ? 0 : 1;
   if (c->precision_mode == PCL_PREC_MIXED) {
     int r = mixed_create(g, x->stream, &x->mixed);
     if (r != PCL_OK) return fail(r);

@@ -326,7 +326,11 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   }
   launch_ghost(g, 1, b->stream);
   launch_timectl(g, kOpInit, 0, 0.0, b->stream);
-  b->launches += 3;
+  launch_metric_check(g, b->stream);
+  b->launches += 4;
+  BCK(cudaMemcpyAsync(&h->nonunit_metric, &g.ctl->nonunit_metric, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  g.unit_metric = h->nonunit_metric ? 0 : 1;
   BCK(cudaMemcpyAsync(b->inst_d + s, &g, sizeof(GridDev), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaGetLastError());
   BCK(cudaStreamSynchronize(b->stream));

@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <algorithm>
+
+#include "pcl_fp64.cuh"
 #include "pcl_ghost.cuh"
 #include "pcl_launch.h"
 #include "pcl_timectl.cuh"
@@ -51,6 +54,30 @@ __global__ void timectl_kernel(GridDev g, int op, int arg, double value) {
 
 void launch_timectl(const GridDev& g, int op, int arg, double value, cudaStream_t st) {
   timectl_kernel<<<1, 1, 0, st>>>(g, op, arg, value);
+}
+
+// ------------------------------------------------------------------------------------------
+// metric check: on grids whose corner coordinates are exact (e.g. 2^k cells on [-1, 1]) every
+// capacity evaluates to exactly 1 and every length ratio is exactly 1; the sweeps then drop
+// the divisions by kappa and the multiplications by gamma, which are exact identities there.
+// ------------------------------------------------------------------------------------------
+__global__ void metric_check_kernel(GridDev g) {
+  const int ni = g.mx + 4, nj = g.my + 4;
+  const long long n = (long long)ni * nj;
+  int bad = 0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % ni) - 1, j = (int)(k / ni) - 1;
+    if (capacity(g.rowm, g.colm, i, j, g.area_scale) != 1.0) bad = 1;
+    if (i == 1 && j >= 1 && j <= g.my && g.rowm[(j + 1) * kRowMetrics + 2] != 1.0) bad = 1;
+    if (j == 1 && i >= 1 && i <= g.mx && g.colm[(i + 1) * kColMetrics + 2] != 1.0) bad = 1;
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&g.ctl->nonunit_metric, 1);
+}
+
+void launch_metric_check(const GridDev& g, cudaStream_t st) {
+  const long long n = (long long)(g.mx + 4) * (g.my + 4);
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+  metric_check_kernel<<<blocks, 256, 0, st>>>(g);
 }
 
 // ------------------------------------------------------------------------------------------

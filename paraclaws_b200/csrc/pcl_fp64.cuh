@@ -129,6 +129,12 @@ __device__ __forceinline__ double corr_coef(double s2, double dtod, double kap_l
   return (0.5 * s2) * (1.0 - (s2 * dtod) / kb);
 }
 
+// corr_coef with kap_l = kap_r = 1: 0.5*(1+1) = 1 and (s2*dtod)/1 = s2*dtod exactly
+__device__ __forceinline__ double corr_coef_unit(double s2, double dtod) {
+  if (s2 == 0.0) return 0.0;
+  return (0.5 * s2) * (1.0 - s2 * dtod);
+}
+
 // Capacity kappa(i,j) of the uniform identity-mapped grid: the shoelace area
 // (domain/SMOD_mesh_manipulation.f90:165-173) reduces to (p1*d + p3*d') / (d_xi*d_eta) with
 // p1 = 0.5*(e1+e1), p3 = 0.5*(e3+e3) per row and d = c1-c2, d' = c2-c1 per column; the two

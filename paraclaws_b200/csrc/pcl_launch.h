@@ -27,5 +27,8 @@ void launch_dam_ic(const GridDev& g, double radius, double h_in, double h_out, d
                    cudaStream_t st);
 void launch_row_sums(const GridDev& g, double* partial /* 3 per interior row */, cudaStream_t st);
 void launch_download(const GridDev& g, double* staging_aos, cudaStream_t st);
+// Sets g.ctl->nonunit_metric (cleared beforehand) when a capacity of cells -1 .. m+2 or an
+// interior length ratio differs from 1.0 as the sweeps compute them.
+void launch_metric_check(const GridDev& g, cudaStream_t st);
 
 }  // namespace pcl

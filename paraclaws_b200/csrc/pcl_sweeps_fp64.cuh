@@ -2,6 +2,10 @@
 // kernels of a single grid (kernels_fp64.cu) and the persistent batched kernel
 // (batch_fp64.cu).  Include only from translation units built with --fmad=false.
 //
+// UM (unit metric): the grid's capacities and length ratios are all exactly 1.0 (checked once
+// per grid by the metric-check kernel), so x/kappa, gamma*x and the capacity mean of the
+// correction coefficient are identities and are left out; the results are the same bits.
+//
 // Buffer rotation replaces solution_old = solution (main.f90:201): the xi sweep reads buffer
 // cur and writes the interior rows of buffer (cur+1)%3; the eta sweep reads those rows plus the
 // pre-step ghost rows of buffer cur (ghosts are filled once per accepted step, main.f90:246) and
@@ -40,7 +44,7 @@ struct XSmem {
   double red[NT / 32];
 };
 
-template <int NT, int LIM, bool SO>
+template <int NT, int LIM, bool SO, bool UM = false>
 __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S) {
   const Ctl* ctl = g.ctl;
   constexpr int L = NT - 4;
@@ -75,7 +79,7 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
       sq[0][t] = h; sq[1][t] = hu; sq[2][t] = hv;
       sf[0][t] = F.f0; sf[1][t] = F.f1; sf[2][t] = F.f2;
       ss[t] = F.s;
-      sk[t] = capacity(g.rowm, g.colm, c, j, g.area_scale);
+      if constexpr (!UM) sk[t] = capacity(g.rowm, g.colm, c, j, g.area_scale);
     }
   }
   __syncthreads();
@@ -117,7 +121,7 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
       if (k <= mx + 1) {
         const int s = t + 1;
         const double s2 = ss2[s];
-        const double cf = corr_coef(s2, dtod, sk[t + 1], sk[t + 2]);
+        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, sk[t + 1], sk[t + 2]);
         if (cf != 0.0) {
           const double w1[3] = {sw1[0][s], sw1[1][s], sw1[2][s]};
           const double w2[3] = {sw2[0][s], sw2[1][s], sw2[2][s]};
@@ -151,8 +155,8 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
     const int i = i0 + t;
     if (i <= mx) {
       const int c = t + 2;
-      const double gam = __ldg(g.rowm + (j + 1) * kRowMetrics + 2);
-      const double dtk = dtod / sk[c];
+      const double gam = UM ? 1.0 : __ldg(g.rowm + (j + 1) * kRowMetrics + 2);
+      const double dtk = UM ? dtod : dtod / sk[c];
       const double sp = ss2[t + 1];       // A+ at interface i:   s2 * W2
       const double sm = -ss2[t + 2];      // A- at interface i+1: s1 * W1
       double* o0 = buffer(g, out) + row;
@@ -160,7 +164,7 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
       for (int me = 0; me < 3; ++me) {
         const double ap = sp * sw2[me][t + 1];
         const double am = sm * sw1[me][t + 2];
-        double q = sq[me][c] - dtk * (gam * ap + gam * am);
+        double q = UM ? sq[me][c] - dtk * (ap + am) : sq[me][c] - dtk * (gam * ap + gam * am);
         if constexpr (SO) q = q - dtk * (sft[me][t + 1] - sft[me][t]);
         o0[me * g.plane + i + 1] = q;
       }
@@ -178,10 +182,10 @@ struct YCell {
   double kap;
 };
 
-template <int LIM, bool SO>
+template <int LIM, bool SO, bool UM>
 __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, const Waves& Wp, double s2,
                                             bool limited, double dtod, double kl, double kr, double ft[3]) {
-  const double cf = corr_coef(s2, dtod, kl, kr);
+  const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, kl, kr);
   if (cf == 0.0) {
     ft[0] = ft[1] = ft[2] = 0.0;
     return;
@@ -201,7 +205,7 @@ __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, con
   for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
 }
 
-template <int LIM, bool SO>
+template <int LIM, bool SO, bool UM = false>
 __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
   Ctl* ctl = g.ctl;
   // xi-sweep validity (MOD_solve.f90:107-120), recomputed here from the reduction word
@@ -225,7 +229,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
   const double* pre = buffer(g, cur);
   const double* xsw = buffer(g, xb);
   double* outp = buffer(g, yb);
-  const double gam = __ldg(g.colm + (ic + 1) * kColMetrics + 2);
+  const double gam = UM ? 1.0 : __ldg(g.colm + (ic + 1) * kColMetrics + 2);
   int bad = 0;
   double smax = 0.0;
 
@@ -238,7 +242,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     int cb = 0;
     c.F = cell_flux<1>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
     if (jj <= my + 1) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
-    c.kap = SO ? capacity(g.rowm, g.colm, ic, jj, g.area_scale) : 1.0;
+    c.kap = (SO && !UM) ? capacity(g.rowm, g.colm, ic, jj, g.area_scale) : 1.0;
   };
   auto iface = [&](int k, const YCell& L, const YCell& R, Waves& W) -> double {
     if (k > my + 1) {
@@ -267,20 +271,20 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     s0 = iface(j0, cm1, cA, W0);
     load(j0 + 1, cB);
     s1 = iface(j0 + 1, cA, cB, W1);
-    if constexpr (SO) y_corr_flux<LIM, SO>(Wm, W0, W1, s0, true, dtod, cm1.kap, cA.kap, ft0);
+    if constexpr (SO) y_corr_flux<LIM, SO, UM>(Wm, W0, W1, s0, true, dtod, cm1.kap, cA.kap, ft0);
   }
   for (int jj = j0; jj <= j1; ++jj) {
     load(jj + 2, cC);
     s2w = iface(jj + 2, cB, cC, W2);
-    if constexpr (SO) y_corr_flux<LIM, SO>(W0, W1, W2, s1, jj + 1 <= my, dtod, cA.kap, cB.kap, ft1);
-    const double kap = SO ? cA.kap : capacity(g.rowm, g.colm, ic, jj, g.area_scale);
-    const double dtk = dtod / kap;
+    if constexpr (SO) y_corr_flux<LIM, SO, UM>(W0, W1, W2, s1, jj + 1 <= my, dtod, cA.kap, cB.kap, ft1);
+    const double kap = (SO || UM) ? cA.kap : capacity(g.rowm, g.colm, ic, jj, g.area_scale);
+    const double dtk = UM ? dtod : dtod / kap;
     const long long o = (long long)(jj + 1) * P + (ic + 1);
 #pragma unroll
     for (int me = 0; me < 3; ++me) {
       const double ap = s0 * W0.w2[me];
       const double am = (-s1) * W1.w1[me];
-      double q = cA.q[me] - dtk * (gam * ap + gam * am);
+      double q = UM ? cA.q[me] - dtk * (ap + am) : cA.q[me] - dtk * (gam * ap + gam * am);
       if constexpr (SO) q = q - dtk * (ft1[me] - ft0[me]);
       if (active) outp[o + me * g.plane] = q;
     }

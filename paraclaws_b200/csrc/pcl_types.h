@@ -63,7 +63,7 @@ struct Ctl {
   int cur;                   // index of the current state buffer (0..2)
   int done;                  // time >= time_final, accepted-step cap reached, or error
   int status;                // kStatus* bits
-  int pad0;
+  int nonunit_metric;        // set by the metric check when some kappa or gamma is not exactly 1
   long long attempts, accepted, max_accepted;
   long long log_cap, log_len;
   StepLogEntry* log;         // optional device log (may be null)
@@ -81,6 +81,7 @@ struct GridDev {
   int mx, my, pitch;
   int bc[4];                 // xi_low, xi_high, eta_low, eta_high (1 wall, 2 zero grad., 3 const. grad.)
   int second_order, limiter; // limiter 0: unlimited correction; 1..4 by code
+  int unit_metric;           // 1: kappa(i,j) == 1 and gamma == 1 exactly on every cell the sweeps read
   double dxi, deta, area_scale /* d_xi*d_eta */, grav;
 };
 
