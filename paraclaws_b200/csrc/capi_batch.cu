@@ -25,7 +25,6 @@ extern "C" void build_tables(const pcl_solver_control* c, double dxi, double det
 namespace {
 
 constexpr long long kBatchLogCap = 8192;
-constexpr int kXSeg = 252;  // cells per FP64 xi-sweep segment (256 threads)
 constexpr int kMixedStrip = 124;
 
 struct Slot {
@@ -78,7 +77,7 @@ struct pcl_batch {
   bool dirty = true;
   int n_items = 0;
   // schedule (the autotuner's knobs)
-  int x_rows = 8, y_rows = 32, tile_rows = 64, blocks_per_sm = 0;
+  int x_rows = 4, y_rows = 16, tile_rows = 64, blocks_per_sm = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   long long launches = 0;
@@ -154,10 +153,11 @@ static int rebuild_items(pcl_batch* b) {
   } else {
     for (int s : order) {
       const auto& c = b->slots[s].cfg;
-      const int nseg = (c.m_xi + kXSeg - 1) / kXSeg;
+      const int xseg = batch_fp64_segment();
+      const int nseg = (c.m_xi + xseg - 1) / xseg;
       int nx = 0;
       for (int j = 1; j <= c.m_eta; j += b->x_rows)
-        for (int k = 0; k < nseg; ++k, ++nx) items.push_back(make_int4(s, kItemX, j, 1 + k * kXSeg));
+        for (int k = 0; k < nseg; ++k, ++nx) items.push_back(make_int4(s, kItemX, j, 1 + k * xseg));
       totals[2 * s] = nx;
     }
     for (int s : order) {

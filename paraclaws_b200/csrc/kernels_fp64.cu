@@ -14,19 +14,25 @@ namespace pcl {
 // launchers
 // ------------------------------------------------------------------------------------------
 namespace {
+// Launch shapes (measured on B200, 4096^2 minmod): the xi sweep at 5 CTAs of 256 threads per SM
+// (48 registers) and the eta sweep at 6 CTAs of 128 threads per SM (80 registers, a few spilled
+// window values) with 16-row strips beat the unconstrained register counts (4 CTAs each) by
+// 20 %: both kernels are latency bound on chains of FP64 divisions and need the warps.
 constexpr int kXT = 256;   // threads (and slots) of an xi-sweep CTA
+constexpr int kXMinBlocks = 5;
 constexpr int kYT = 128;   // columns of an eta-sweep CTA
-constexpr int kYS = 32;    // rows of an eta-sweep strip
+constexpr int kYMinBlocks = 6;
+constexpr int kYS = 16;    // rows of an eta-sweep strip
 
 template <int NT, int LIM, bool SO, bool UM>
-__global__ void __launch_bounds__(NT) xsweep_fp64_kernel(GridDev g) {
+__global__ void __launch_bounds__(NT, kXMinBlocks) xsweep_fp64_kernel(GridDev g) {
   __shared__ XSmem<NT> S;
   if (g.ctl->done) return;
   xsweep_segment<NT, LIM, SO, UM>(g, 1 + blockIdx.y, 1 + blockIdx.x * (NT - 4), S);
 }
 
 template <int NTX, int STRIP, int LIM, bool SO, bool UM>
-__global__ void __launch_bounds__(NTX) ysweep_fp64_kernel(GridDev g) {
+__global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g) {
   if (g.ctl->done) return;
   ysweep_strip<LIM, SO, UM>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
 }

@@ -33,7 +33,8 @@ struct BatchView {
 
 void launch_batch_fp64(const BatchView& v, int grid, cudaStream_t st);
 void launch_batch_mixed(const BatchView& v, int grid, cudaStream_t st);
-int batch_fp64_threads();
+int batch_fp64_threads();   // also the columns of an FP64 eta item
+int batch_fp64_segment();   // cells of an FP64 xi item's row segment
 int batch_mixed_threads();
 // largest number of resident CTAs per SM of each persistent kernel
 int batch_fp64_occupancy();

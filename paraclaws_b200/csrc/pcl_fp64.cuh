@@ -26,17 +26,47 @@ struct CellFlux {
   double f0, f1, f2, s;
 };
 
+// IEEE division with the zero-numerator case answered without dividing.  CUDA's correctly
+// rounded double division leaves its fast path for a zero (or tiny) numerator, and a warp pays
+// that path when any lane takes it; quiescent cells (zero momentum) make such numerators
+// common.  For a = +-0 the quotient is an exact signed zero: a / b = a for b > 0 (+inf
+// included) and -a for b < 0.  Every other case divides, so the result is the same bits as
+// a / b for all inputs (b = 0 or NaN still divides and gives NaN).  The numerator select is
+// inline PTX so that the optimiser cannot fold it back into the division.
+__device__ __forceinline__ double numerator_or_one(double a, bool use_one) {
+  double r;
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %2, 0;\n\tselp.f64 %0, 0d3FF0000000000000, %1, p;\n\t}"
+      : "=d"(r)
+      : "d"(a), "r"((int)use_one));
+  return r;
+}
+__device__ __forceinline__ double div_pos_den(double a, double b) {  // quotient for b > 0
+  const bool z = a == 0.0 && b > 0.0;
+  const double q = numerator_or_one(a, z) / b;
+  return z ? a : q;
+}
+__device__ __forceinline__ double div_neg_den(double a, double b) {  // quotient for b < 0
+  const bool z = a == 0.0 && b < 0.0;
+  const double q = numerator_or_one(a, z) / b;
+  return z ? -a : q;
+}
+
 template <int DIR>
 __device__ __forceinline__ CellFlux cell_flux(double h, double hu, double hv, double g, int* bad) {
   const double n = DIR == 0 ? hu : hv;
   const double hh = h * h;
-  const double d1 = (n * n) / hh;
-  const double d3 = (hu * hv) / hh;
-  const double d4 = hv / h;
-  const double d5 = hu / h;
+  const double d1 = div_pos_den(n * n, hh);
+  const double d3 = div_pos_den(hu * hv, hh);
+  const double d4 = div_pos_den(hv, h);
+  const double d5 = div_pos_den(hu, h);
   const double un = DIR == 0 ? d5 : d4;
-  // (2n)/h == 2*(n/h) exactly unless n/h is subnormal (scaling by 2 commutes with rounding)
-  const double d2 = fabs(un) >= 0x1p-1000 ? 2.0 * un : (2.0 * n) / h;
+  // (2n)/h == 2*(n/h) exactly unless n/h is subnormal (scaling by 2 commutes with rounding);
+  // a branch, so the rare division is not evaluated for every cell
+  double d2;
+  if (fabs(un) >= 0x1p-1000)
+    d2 = 2.0 * un;
+  else
+    d2 = div_pos_den(2.0 * n, h);
   const double gh = g * h;
   const double jn = -d1 + gh;
   const double jt = -d3;
@@ -72,7 +102,7 @@ __device__ __forceinline__ double hll(const double qL[3], const CellFlux& fL, co
     const double fr[3] = {fR.f0, fR.f1, fR.f2};
 #pragma unroll
     for (int me = 0; me < 3; ++me) {
-      const double qs = (((fr[me] - fl[me]) - smax * qR[me]) + s1 * qL[me]) / den;
+      const double qs = div_neg_den(((fr[me] - fl[me]) - smax * qR[me]) + s1 * qL[me], den);
       W.w1[me] = qs - qL[me];
       W.w2[me] = qR[me] - qs;
     }
@@ -91,7 +121,7 @@ template <int LIM>
 __device__ __forceinline__ double limiter_phi(double r) {
   if (LIM == 1) return fmax(0.0, fmin(1.0, r));
   if (LIM == 2) return fmax(fmax(0.0, fmin(1.0, 2.0 * r)), fmin(2.0, r));
-  if (LIM == 3) return (r + fabs(r)) / (1.0 + fabs(r));
+  if (LIM == 3) return div_pos_den(r + fabs(r), 1.0 + fabs(r));  // zero numerator for every r <= 0
   return fmax(0.0, fmin(fmin((1.0 + r) / 2.0, 2.0), 2.0 * r));
 }
 
@@ -115,7 +145,7 @@ __device__ __forceinline__ void limit_wave(const double wm[3], const double w[3]
     return;
   }
   const double up = lambda_pos ? dot3(wm, w) : dot3(w, wp);
-  const double phi = limiter_phi<LIM>(up / wn2);
+  const double phi = limiter_phi<LIM>(div_pos_den(up, wn2));
   out[0] = phi * w[0];
   out[1] = phi * w[1];
   out[2] = phi * w[2];
