@@ -15,7 +15,7 @@ __global__ void __launch_bounds__(NT) fused_mixed_kernel(GridDev g, int TY, int 
   if (g.ctl->done) return;
   init_ring(S);
   unsigned rows = 0;
-  mixed_item<LIM, SO>(g, blockIdx.x % nstrips, blockIdx.x / nstrips, TY, S, rows);
+  mixed_item<LIM, SO, 2>(g, blockIdx.x % nstrips, blockIdx.x / nstrips, TY, S, rows);
 }
 
 struct Workspace {

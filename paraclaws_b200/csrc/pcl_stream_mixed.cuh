@@ -65,14 +65,11 @@ struct WF {
   float w1[3], w2[3];
 };
 
-// HLL in jump form; components in (h, n, t) order.  Returns s2 (0 for a degenerate interface).
+// HLL in jump form; components in (h, n, t) order.  Returns s2 (0 for a degenerate interface,
+// whose waves are 0).  Branch-free: the degenerate case is selected after the arithmetic.
 __device__ __forceinline__ float hll_m(const CellM& L, const CellM& R, const float dq[3], float g, WF& W) {
   const float s2 = fmaxf(L.s, R.s);
-  if (!(s2 > kEps)) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) W.w1[k] = W.w2[k] = 0.f;
-    return 0.f;
-  }
+  const bool live = s2 > kEps;
   const float du = __fmaf_rn(dq[1], L.h, -(L.n * dq[0])) * (L.ih * R.ih);
   const float gsum = g * (L.h + R.h);
   const float df[3] = {dq[1], __fmaf_rn(R.un, dq[1], __fmaf_rn(L.n, du, gsum * dq[0])),
@@ -81,10 +78,11 @@ __device__ __forceinline__ float hll_m(const CellM& L, const CellM& R, const flo
   const float rden = __fdividef(1.f, (kEps - s2) - s2);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    W.w1[k] = __fmaf_rn(-kEps, ql[k], __fmaf_rn(-s2, dq[k], df[k])) * rden;
-    W.w2[k] = dq[k] - W.w1[k];
+    const float w1 = __fmaf_rn(-kEps, ql[k], __fmaf_rn(-s2, dq[k], df[k])) * rden;
+    W.w1[k] = live ? w1 : 0.f;
+    W.w2[k] = live ? dq[k] - w1 : 0.f;
   }
-  return s2;
+  return live ? s2 : 0.f;
 }
 
 template <int LIM>
@@ -99,11 +97,14 @@ __device__ __forceinline__ float dot3f(const float a[3], const float b[3]) {
   return __fmaf_rn(a[0], b[0], __fmaf_rn(a[1], b[1], a[2] * b[2]));
 }
 
+// wave limited by phi(theta), theta = upstream / |W|^2; phi = 1 where |W|^2 <= eps or where the
+// interface is not limited (1 * w == w).  Branch-free.
 template <int LIM>
-__device__ __forceinline__ void limit_f(const float wm[3], const float w[3], const float wp[3], bool pos, float o[3]) {
+__device__ __forceinline__ void limit_f(const float wm[3], const float w[3], const float wp[3], bool pos, bool limited,
+                                        float o[3]) {
   const float wn2 = dot3f(w, w);
-  float ph = 1.f;
-  if (wn2 > kEps) ph = phi_f<LIM>(__fdividef(pos ? dot3f(wm, w) : dot3f(w, wp), wn2));
+  const float r = __fdividef(pos ? dot3f(wm, w) : dot3f(w, wp), wn2);
+  const float ph = limited && wn2 > kEps ? phi_f<LIM>(r) : 1.f;
 #pragma unroll
   for (int k = 0; k < 3; ++k) o[k] = ph * w[k];
 }
@@ -112,15 +113,15 @@ __device__ __forceinline__ void limit_f(const float wm[3], const float w[3], con
 template <int LIM, bool SO>
 __device__ __forceinline__ void corr_f(const WF& Wm, const WF& W, const WF& Wp, float s2, bool limited, float dtodf,
                                        float ft[3]) {
-  if (!SO || s2 == 0.f) {
+  if (!SO) {
     ft[0] = ft[1] = ft[2] = 0.f;
     return;
   }
   const float cf = (0.5f * s2) * __fmaf_rn(-s2, dtodf, 1.f);
   float a[3], b[3];
-  if (LIM != 0 && limited) {
-    limit_f<LIM>(Wm.w1, W.w1, Wp.w1, false, a);
-    limit_f<LIM>(Wm.w2, W.w2, Wp.w2, true, b);
+  if (LIM != 0) {
+    limit_f<LIM>(Wm.w1, W.w1, Wp.w1, false, limited, a);
+    limit_f<LIM>(Wm.w2, W.w2, Wp.w2, true, limited, b);
   } else {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -128,8 +129,9 @@ __device__ __forceinline__ void corr_f(const WF& Wm, const WF& W, const WF& Wp, 
       b[k] = W.w2[k];
     }
   }
+  const bool live = s2 != 0.f;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) ft[k] = cf * (a[k] + b[k]);
+  for (int k = 0; k < 3; ++k) ft[k] = live ? cf * (a[k] + b[k]) : 0.f;
 }
 
 // Shared memory of one CTA.  Per-slot data of the xi sweep is packed in float4 so a neighbour's
@@ -154,7 +156,10 @@ __device__ __forceinline__ WF load_wf(const Smem& S, int s) {
 // streamed through the ring before this item (slot and mbarrier parity continue across items);
 // the item's wave-speed maxima and status bits go to g.ctl before it returns.  All threads of
 // the CTA call it together.  Returns false if a bulk copy did not arrive in time.
-template <int LIM, bool SO>
+// UNROLL unrolls the row loop (the single-grid kernel: 2, letting the eta window shift by
+// renaming; the batched kernel: 1, which keeps its register count at four CTAs per SM).  It
+// changes no arithmetic.
+template <int LIM, bool SO, int UNROLL = 1>
 __device__ __forceinline__ bool mixed_item(const GridDev& g, int strip, int seg, int TY, Smem& S, unsigned& rows) {
   Ctl* ctl = g.ctl;
   const int t = threadIdx.x;
@@ -201,7 +206,10 @@ __device__ __forceinline__ bool mixed_item(const GridDev& g, int strip, int seg,
   bool timed_out = false;
   int issued = min(AHEAD, nrows), consumed = 0;
   const int tc = t + 2 < NT ? t + 2 : NT - 1;  // ring slot of this thread's column
+  const int t1 = t + 1 < NT ? t + 1 : NT - 1;  // next slot (clamped)
+  const int t2 = tc;                           // slot after next (clamped)
 
+#pragma unroll UNROLL
   for (int k = 0; k < nrows; ++k) {
     const int jr = jfirst + k;
     const unsigned kk = base + k;
@@ -223,48 +231,53 @@ __device__ __forceinline__ bool mixed_item(const GridDev& g, int strip, int seg,
 
     if (jr >= 1 && jr <= my) {
       // ---- xi sweep of row jr ----
+      // Branch-free phases: every thread computes, results outside the valid range are
+      // selected to zero (or never read); slot indices past the row are clamped.
       const int c = i0 - 2 + t;  // phase A: this thread's cell (slot t)
       const double qm[3] = {r0[t], r1[t], r2[t]};
-      CellM me{};
-      if (c <= mx + 2) {
-        me = cell_m(qm[0], qm[1], qm[2], gf);
-        if (c <= mx + 1) bad |= bad_m(me, qm[0]);
-        S.cA[t] = make_float4(me.h, me.n, me.t, me.ih);
-        S.cB[t] = make_float2(me.un, me.s);
-      }
+      const CellM me = cell_m(qm[0], qm[1], qm[2], gf);
+      if (c <= mx + 1) bad |= bad_m(me, qm[0]);
+      S.cA[t] = make_float4(me.h, me.n, me.t, me.ih);
+      S.cB[t] = make_float2(me.un, me.s);
       __syncthreads();
-      WF Wme{};  // phase B: interface i0-1+t between slots t (own) and t+1
-      float s2me = 0.f;
-      if (t < NT - 1) {
-        if (i0 - 1 + t <= mx + 1) {
-          const float4 a = S.cA[t + 1];
-          const float2 b = S.cB[t + 1];
-          const CellM R = {a.x, a.y, a.z, a.w, b.x, b.y};
-          const float dq[3] = {(float)(r0[t + 1] - qm[0]), (float)(r1[t + 1] - qm[1]), (float)(r2[t + 1] - qm[2])};
-          s2me = hll_m(me, R, dq, gf, Wme);
-          smx = fmaxf(smx, s2me);
+      WF Wme;  // phase B: interface i0-1+t between slots t (own) and t+1
+      float s2me;
+      {
+        const float4 a = S.cA[t1];
+        const float2 b = S.cB[t1];
+        const CellM R = {a.x, a.y, a.z, a.w, b.x, b.y};
+        const float dq[3] = {(float)(r0[t1] - qm[0]), (float)(r1[t1] - qm[1]), (float)(r2[t1] - qm[2])};
+        s2me = hll_m(me, R, dq, gf, Wme);
+        const bool v = t < NT - 1 && i0 - 1 + t <= mx + 1;
+        s2me = v ? s2me : 0.f;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          Wme.w1[q] = v ? Wme.w1[q] : 0.f;
+          Wme.w2[q] = v ? Wme.w2[q] : 0.f;
         }
+        smx = fmaxf(smx, s2me);
         S.wA[t] = make_float4(Wme.w1[0], Wme.w1[1], Wme.w1[2], s2me);
         S.wB[t] = make_float4(Wme.w2[0], Wme.w2[1], Wme.w2[2], 0.f);
       }
       __syncthreads();
       float ftme[3] = {0.f, 0.f, 0.f};  // phase C: correction flux at interface i0+t (slot t+1)
-      if (SO && t < NT - 3) {
+      if (SO) {
         const int kf = i0 + t;
-        if (kf <= mx + 1) {
-          const WF W0 = load_wf(S, t + 1);
-          const WF Wp = load_wf(S, t + 2);
-          corr_f<LIM, SO>(Wme, W0, Wp, S.wA[t + 1].w, kf <= mx, dtodxf, ftme);
-        }
+        const WF W0 = load_wf(S, t1);
+        const WF Wp = load_wf(S, t2);
+        corr_f<LIM, SO>(Wme, W0, Wp, S.wA[t1].w, kf <= mx, dtodxf, ftme);
+        const bool v = t < NT - 3 && kf <= mx + 1;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) ftme[q] = v ? ftme[q] : 0.f;
         S.ft[t] = make_float4(ftme[0], ftme[1], ftme[2], 0.f);
+        __syncthreads();
       }
-      if (SO) __syncthreads();
-      if (ycol) {  // phase D: x-swept value of this thread's column
-        const float4 a = S.wA[t + 1], b = S.wB[t + 1], d = S.wA[t + 2];
+      {  // phase D: x-swept value of this thread's column (used only where ycol)
+        const float4 a = S.wA[t1], b = S.wB[t1], d = S.wA[t2];
         const float sp = a.w, sm = -d.w;
         float fs[3] = {__fmaf_rn(sp, b.x, sm * d.x), __fmaf_rn(sp, b.y, sm * d.y), __fmaf_rn(sp, b.z, sm * d.z)};
         if (SO) {
-          const float4 f1 = S.ft[t + 1];
+          const float4 f1 = S.ft[t1];
           fs[0] += f1.x - ftme[0];
           fs[1] += f1.y - ftme[1];
           fs[2] += f1.z - ftme[2];
