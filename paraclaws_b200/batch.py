@@ -135,7 +135,7 @@ class Batch:
 # ------------------------------------------------------------------------------------------
 def candidate_schedules(precision: int) -> List[Schedule]:
     if precision == PRECISION_MIXED:
-        return [Schedule(tile_rows=tr, blocks_per_sm=b) for tr in (16, 32, 64, 128) for b in (0, 2, 3)]
+        return [Schedule(tile_rows=tr, blocks_per_sm=b) for tr in (32, 64, 128, 256) for b in (0, 3)]
     return [Schedule(x_rows=xr, y_rows=yr, blocks_per_sm=b) for xr in (2, 4, 8) for yr in (8, 16, 32) for b in (0, 4)]
 
 
