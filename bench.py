@@ -265,6 +265,54 @@ def form_mixed(m, steps, warmup, device, fp64_value):
             "ms_per_step": ms / max(steps, 1)}
 
 
+def skewed_metrics(m: int):
+    """Capacity and face length ratios of the skewed mapping x = xi + 0.1 sin(pi eta),
+    y = eta + 0.08 xi^2 on the m^2 grid of [-1, 1]^2, vectorised (finalize_mesh's formulas; the
+    timing does not depend on the last bits)."""
+    import numpy as np
+    d = 2.0 / m
+    i = np.arange(-1, m + 3, dtype=np.float64)
+    xi1 = -1.0 + (i - 1) * d
+    eta1 = xi1.copy()
+    X1, Y1 = np.meshgrid(xi1, eta1)
+    corners = [(X1, Y1), (X1 + d, Y1), (X1 + d, Y1 + d), (X1, Y1 + d), (X1, Y1)]
+    pts = [(a + 0.1 * np.sin(np.pi * b), b + 0.08 * a * a) for a, b in corners]
+    lrx = np.hypot(pts[3][0] - pts[0][0], pts[3][1] - pts[0][1]) / d
+    lry = np.hypot(pts[1][0] - pts[0][0], pts[1][1] - pts[0][1]) / d
+    area = np.zeros_like(X1)
+    for k in range(4):
+        area = area + (0.5 * (pts[k][1] + pts[k + 1][1])) * (pts[k][0] - pts[k + 1][0])
+    return area / (d * d), lrx, lry
+
+
+def form_mapped(m, steps, warmup, device, fp64_value):
+    """FP64 path on a mapped grid: the plain-large workload with per-cell capacity and face
+    length ratios of a skewed curvilinear mapping (2 x 16 B more reads per cell-update)."""
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200 import ic
+    from paraclaws_b200.solver import Solver
+    c = workload(m)
+    q = ic.gaussian_bumps(m, m, seed=0)
+    s = Solver(c, ctl.CustomSettings(max_accepted_steps=steps), device=device)
+    s.set_mesh_metrics(*skewed_metrics(m))
+    s.upload(q)
+    s.update_rank_boundaries()
+    s.advance(max_attempts=warmup)
+    s.upload(q)
+    s.update_rank_boundaries()
+    s.reset_time_control()
+    st, ms = _timed_advance(s, steps, torch)
+    value = st.accepted * m * m / (ms * 1e-3)
+    peak, _ = hbm_peak()
+    s.close()
+    return {"value": value, "unit": UNIT, "vs_uniform_fp64": value / fp64_value, "ms_per_step": ms / max(steps, 1),
+            "algorithmic_bytes_per_cell_update": 128,
+            "roofline_frac": value * 128 / 1e9 / peak,
+            "workload": f"{m}^2 bumps (seed 0), minmod, mapping x = xi + 0.1 sin(pi eta), y = eta + 0.08 xi^2"}
+
+
 def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 300, 400, 500, 700, 1000)):
     """Precision-form accuracy on the 8192^2 seeded dam break, 1000 accepted steps: the mixed
     form against FP64 at checkpoints, beside the conditioning floor of the step itself -- FP64
@@ -374,17 +422,57 @@ def form_batch(device, n=512, steps=32):
     return res
 
 
-def form_serving(device):
-    """Poisson arrivals, sides log-uniform 128..2048, end time U(0.1, 1), 120 GB budget."""
+def form_serving(device, l1_sample: int = 8):
+    """Poisson arrivals, sides log-uniform 128..2048, end time U(0.1, 1), 120 GB budget.  Mixed is
+    swept over arrival rates from partial load to saturation; at the middle rate the first
+    `l1_sample` served results are compared with the same solves run alone in FP64."""
+    import numpy as np
+
     from paraclaws_b200 import control as ctl
     from paraclaws_b200.serve import SolveServer, poisson_requests
-    res = {}
-    for name, prec, n, rate in (("mixed", ctl.PRECISION_MIXED, 80, 12.0), ("fp64", ctl.PRECISION_FP64, 30, 3.0)):
+    from paraclaws_b200.solver import Solver
+    res = {"mixed": [], "fp64": []}
+    runs = [("mixed", ctl.PRECISION_MIXED, 40, 4.0), ("mixed", ctl.PRECISION_MIXED, 80, 12.0),
+            ("mixed", ctl.PRECISION_MIXED, 120, 24.0), ("fp64", ctl.PRECISION_FP64, 30, 3.0)]
+    for name, prec, n, rate in runs:
+        keep = name == "mixed" and rate == 12.0
         reqs = poisson_requests(n, rate=rate, seed=3, precision=prec)
-        srv = SolveServer(precision=prec, budget_bytes=120e9, max_slots=512, steps_per_tick=16, device=device)
+        srv = SolveServer(precision=prec, budget_bytes=120e9, max_slots=512, steps_per_tick=16, device=device,
+                          keep_states=keep)
         rep = srv.run(reqs, max_wall=240.0)
         srv.close()
-        res[name] = {"rate_per_s": rate, **rep.summary()}
+        entry = {"rate_per_s": rate, **rep.summary()}
+        if keep:
+            rows = []
+            rng = np.random.Generator(np.random.PCG64(7))
+            for r in sorted(rep.results, key=lambda r: r.rid)[:l1_sample]:
+                rq = reqs[r.rid]
+                cu = ctl.CustomSettings(**{**rq.custom.__dict__, "precision_mode": ctl.PRECISION_FP64})
+                finals = []
+                for perturb in (False, True):
+                    sv = Solver(rq.control, cu, device=device, precision=ctl.PRECISION_FP64)
+                    sv.initial_condition()
+                    if perturb:  # the same start with h raised by one ulp in 1% of the cells
+                        q0 = sv.download()
+                        mask = rng.random(q0.shape[:2]) < 0.01
+                        q0[..., 0] = np.where(mask, np.nextafter(q0[..., 0], np.inf), q0[..., 0])
+                        sv.upload(q0)
+                    sv.update_rank_boundaries()
+                    st = sv.advance()
+                    finals.append(sv.download()[2:-2, 2:-2, 0])
+                    sv.close()
+                ref, pert = finals
+                got = r.state[2:-2, 2:-2, 0]
+                scale = float(np.abs(ref).sum())
+                rows.append({"side": rq.control.m_xi, "t_end": rq.control.time_final, "steps": int(st.accepted),
+                             "l1_h": float(np.abs(got - ref).sum() / scale),
+                             "fp64_floor_l1_h": float(np.abs(pert - ref).sum() / scale)})
+            l1 = [x["l1_h"] for x in rows]
+            entry["l1_h_vs_solo_fp64"] = {"sample": len(rows), "median": float(np.median(l1)), "max": float(max(l1)),
+                                          "requests": rows,
+                                          "note": "fp64_floor_l1_h: FP64 against FP64 from the same start with h "
+                                                  "+1 ulp in 1% of the cells (the step's own amplification)"}
+        res[name].append(entry)
     return res
 
 # ------------------------------------------------------------------------------------------
@@ -521,6 +609,7 @@ def run_ours(args) -> None:
         line["cpu_baseline"] = cpu_baseline(m)
     if rank == 0 and world == 1 and not args.no_forms:
         line["forms"] = {"mixed": form_mixed(m, args.steps, args.warmup, local, value),
+                         "mapped": form_mapped(m, min(args.steps, 200), args.warmup, local, value),
                          "batch": form_batch(local),
                          "serving": form_serving(local),
                          "precision": form_precision(local)}

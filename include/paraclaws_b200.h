@@ -107,6 +107,33 @@ int pcl_download_state(pcl_ctx* ctx, double* vars);
    hu = hv = 0, on the whole padded block.  Needs initial_condition = 1. */
 int pcl_initial_condition(pcl_ctx* ctx);
 
+/* ---- mapped (curvilinear) grids ---- */
+
+/* Mesh metrics of a mapped grid, as finalize_mesh leaves them in the reference
+   (domain/SMOD_mesh_manipulation.f90:147-173; MOD_domain.f90:68-78): capacity(i,j),
+   length_ratio_xi(1,i,j) (the xi face between cells i-1 and i) and length_ratio_eta(1,i,j) (the
+   eta face between cells j-1 and j), each a column-major (m_xi+4) x (m_eta+4) array with lower
+   bounds -1, i.e. the reference's own arrays.  The FP64 sweeps then read them per cell
+   (solver/MOD_solve.f90:211-233, MOD_flux_correction.f90:162-181).  A Fortran host passes the
+   arrays its finalize_mesh computed.  FP64 contexts only (PCL_ERR_BADARG otherwise).  The
+   device dam-break initial condition (pcl_initial_condition) uses computational coordinates;
+   a mapped grid's initial state is uploaded by the host. */
+int pcl_set_mesh_metrics(pcl_ctx* ctx, const double* capacity, const double* length_ratio_xi,
+                         const double* length_ratio_eta);
+
+/* map_to_physical_coordinates (user_subroutines/SMOD_coordinate_mapping.f90:35-43): (xi, eta) ->
+   (x, y). */
+typedef void (*pcl_map_fn)(double xi, double eta, double* x, double* y, void* user);
+
+/* The three metric arrays of pcl_set_mesh_metrics computed on the host from a coordinate mapping
+   (NULL: the identity), in the reference's order: corners of initialize_computational_coordinates
+   (SMOD_mesh_manipulation.f90:14-56), face length ratio NORM2(face)/delta and the shoelace area
+   over delta_xi*delta_eta.  NORM2 of a face vector (a, b) is |a| when b = 0, |b| when a = 0 and
+   sqrt(a*a + b*b) otherwise (the Fortran intrinsic's rounding on skewed faces is
+   compiler-defined).  Outputs as in pcl_set_mesh_metrics.  Allocates nothing on the device. */
+int pcl_compute_mesh_metrics(const pcl_solver_control* ctl, pcl_map_fn map, void* user, double* capacity,
+                             double* length_ratio_xi, double* length_ratio_eta);
+
 /* ---- the hot path, one call per reference routine ---- */
 
 /* update_rank_boundaries (user_subroutines/SMOD_boundary_conditions.f90:17-56): on-device

@@ -741,6 +741,14 @@ void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double
     if (lr_eta) memcpy(lr_eta, o->lr_eta, n);
 }
 
+void orc_set_mesh(orc_t* o, const double* kappa, const double* lr_xi, const double* lr_eta)
+{
+    const size_t n = sizeof(double) * (size_t)o->ni * (size_t)o->nj;
+    memcpy(o->kappa, kappa, n);
+    memcpy(o->lr_xi, lr_xi, n);
+    memcpy(o->lr_eta, lr_eta, n);
+}
+
 int orc_update_time(orc_t* o, int step_valid) { return tctl_update_time(&o->t, step_valid); }
 void orc_reset_cfl(orc_t* o)
 {

@@ -63,6 +63,9 @@ void orc_get_state(const orc_t* o, double* vars);
 
 /* mesh metrics (same padded layout, one value per cell) */
 void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double* lr_xi, double* lr_eta);
+/* replace capacity and face length ratios by those of a mapped grid (finalize_mesh of a user
+   mapping, SMOD_mesh_manipulation.f90:147-173); cell centres stay computational */
+void orc_set_mesh(orc_t* o, const double* kappa, const double* lr_xi, const double* lr_eta);
 
 int    orc_update_rank_boundaries(orc_t* o);
 int    orc_solve_dimensional_split(orc_t* o, int* ierr);

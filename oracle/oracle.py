@@ -66,6 +66,7 @@ def lib():
         L.orc_set_state.argtypes = [C.c_void_p, dp]
         L.orc_get_state.argtypes = [C.c_void_p, dp]
         L.orc_get_mesh.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
+        L.orc_set_mesh.argtypes = [C.c_void_p, dp, dp, dp]
         L.orc_update_rank_boundaries.argtypes = [C.c_void_p]
         L.orc_solve_dimensional_split.argtypes = [C.c_void_p, P(C.c_int)]
         L.orc_sweep.argtypes = [C.c_void_p, C.c_int, P(C.c_double)]
@@ -176,6 +177,14 @@ class Oracle:
         arrs = [np.empty(n, dtype=np.float64) for _ in range(5)]
         lib().orc_get_mesh(self.h, *arrs)
         return dict(zip(["xi", "eta", "kappa", "lr_xi", "lr_eta"], arrs))
+
+    def set_mesh(self, kappa, lr_xi, lr_eta) -> None:
+        """Metrics of a mapped grid (arrays shaped like mesh()['kappa'])."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (kappa, lr_xi, lr_eta)]
+        for a in arrs:
+            if a.shape != self.shape[:2]:
+                raise ValueError(f"metric shape {a.shape} != {self.shape[:2]}")
+        lib().orc_set_mesh(self.h, *arrs)
 
     def status(self) -> int:
         return lib().orc_status(self.h)

@@ -100,6 +100,8 @@ def load(build_if_missing: bool = True):
                  "pcl_reset_cfl", "pcl_advance_snapshot_index", "pcl_synchronize"):
         getattr(L, name).argtypes = [vp]
     L.pcl_solve_dimensional_split.argtypes = [vp, P(C.c_int)]
+    L.pcl_set_mesh_metrics.argtypes = [vp, vp, vp, vp]
+    L.pcl_compute_mesh_metrics.argtypes = [P(SolverControl), vp, vp, vp, vp, vp]
     L.pcl_update_time.argtypes = [vp, C.c_int]
     L.pcl_set_dt.argtypes = [vp, C.c_double]
     for name in ("pcl_get_time", "pcl_get_dt", "pcl_get_previous_dt", "pcl_get_cfl"):
@@ -156,6 +158,10 @@ def check(code: int, where: str) -> int:
     if code < 0:
         raise PclError(code, where)
     return code
+
+
+# pcl_map_fn: void (*)(double xi, double eta, double* x, double* y, void* user)
+MapFn = C.CFUNCTYPE(None, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
 
 
 def declared_functions() -> list:

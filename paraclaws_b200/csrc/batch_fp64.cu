@@ -22,37 +22,38 @@ namespace {
 constexpr int kThreads = 128;
 constexpr int kMinBlocks = 6;
 
-template <int LIM, bool SO, bool UM>
+template <int LIM, bool SO, int MK>
 __device__ __forceinline__ void run_item(const GridDev& g, int kind, int a, int b, const BatchView& v,
                                          XSmem<kThreads>& S) {
   if (kind == kItemX) {
     const int jend = min(a + v.x_rows - 1, g.my);
     for (int j = a; j <= jend; ++j) {
-      xsweep_segment<kThreads, LIM, SO, UM>(g, j, b, S);
+      xsweep_segment<kThreads, LIM, SO, MK>(g, j, b, S);
       __syncthreads();  // the segment's shared arrays are reused by the next row
     }
   } else {
-    ysweep_strip<LIM, SO, UM>(g, a, b, v.y_rows);
+    ysweep_strip<LIM, SO, MK>(g, a, b, v.y_rows);
   }
 }
 
-template <bool UM>
+template <int MK>
 __device__ __forceinline__ void dispatch_lim(const GridDev& g, int kind, int a, int b, const BatchView& v,
                                              XSmem<kThreads>& S) {
-  if (!g.second_order) return run_item<0, false, UM>(g, kind, a, b, v, S);
+  if (!g.second_order) return run_item<0, false, MK>(g, kind, a, b, v, S);
   switch (g.limiter) {
-    case 1: return run_item<1, true, UM>(g, kind, a, b, v, S);
-    case 2: return run_item<2, true, UM>(g, kind, a, b, v, S);
-    case 3: return run_item<3, true, UM>(g, kind, a, b, v, S);
-    case 4: return run_item<4, true, UM>(g, kind, a, b, v, S);
-    default: return run_item<0, true, UM>(g, kind, a, b, v, S);
+    case 1: return run_item<1, true, MK>(g, kind, a, b, v, S);
+    case 2: return run_item<2, true, MK>(g, kind, a, b, v, S);
+    case 3: return run_item<3, true, MK>(g, kind, a, b, v, S);
+    case 4: return run_item<4, true, MK>(g, kind, a, b, v, S);
+    default: return run_item<0, true, MK>(g, kind, a, b, v, S);
   }
 }
 
 __device__ __forceinline__ void dispatch_item(const GridDev& g, int kind, int a, int b, const BatchView& v,
                                               XSmem<kThreads>& S) {
-  if (g.unit_metric) return dispatch_lim<true>(g, kind, a, b, v, S);
-  return dispatch_lim<false>(g, kind, a, b, v, S);
+  // batched instances are uniform grids (pcl_batch_add builds the row/column tables)
+  if (g.metric == kMetricUnit) return dispatch_lim<kMetricUnit>(g, kind, a, b, v, S);
+  return dispatch_lim<kMetricTable>(g, kind, a, b, v, S);
 }
 
 __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchView v) {

@@ -27,6 +27,7 @@ struct pcl_ctx {
   Ctl* ctl_h = nullptr;          // pinned mirror for reads
   double* bufs_d = nullptr;      // 3 state buffers
   double* tables_d = nullptr;    // row + column metric tables
+  double* metrics_d = nullptr;   // mapped grids: capacity and face length ratios per cell
   double* staging_d = nullptr;   // AoS staging for upload/download
   StepLogEntry* log_d = nullptr;
   long long log_cap = 0;
@@ -283,6 +284,7 @@ static void free_ctx(pcl_ctx* x) {
   if (x->mixed) mixed_free(x->mixed);
   cudaFree(x->bufs_d);
   cudaFree(x->tables_d);
+  cudaFree(x->metrics_d);
   cudaFree(x->staging_d);
   cudaFree(x->ctl_d);
   cudaFree(x->log_d);
@@ -355,7 +357,7 @@ int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
   if (cudaMemcpyAsync(&x->ctl_h->nonunit_metric, &g.ctl->nonunit_metric, sizeof(int), cudaMemcpyDeviceToHost,
                       x->stream) != cudaSuccess || cudaStreamSynchronize(x->stream) != cudaSuccess)
     return fail(PCL_ERR_CUDA);
-  g.unit_metric = x->ctl_h->nonunit_metric ? 0 : 1;
+  g.metric = x->ctl_h->nonunit_metric ? kMetricTable : kMetricUnit;
   if (c->precision_mode == PCL_PREC_MIXED) {
     int r = mixed_create(g, x->stream, &x->mixed);
     if (r != PCL_OK) return fail(r);
@@ -698,14 +700,85 @@ int pcl_conservation_sums(pcl_ctx* x, double* sums) {
   return PCL_OK;
 }
 
-int pcl_set_tile_rows(pcl_ctx* x, int rows) {
-  if (!x || rows < 4) return PCL_ERR_BADARG;
-  if (x->mixed) mixed_set_tile_rows(x->mixed, rows);
-  if (x->graph) {  // the captured launches carry the old tiling
+static void drop_graph(pcl_ctx* x) {
+  if (x->graph) {  // the captured launches carry the old kernels
     cudaGraphExecDestroy(x->graph);
     x->graph = nullptr;
     x->graph_chunk = 0;
   }
+}
+
+int pcl_set_mesh_metrics(pcl_ctx* x, const double* capacity, const double* lrx, const double* lry) {
+  if (!x || !capacity || !lrx || !lry || x->cfg.precision_mode != PCL_PREC_FP64) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  GridDev& g = x->g;
+  const size_t ni = (size_t)g.mx + 4, nj = (size_t)g.my + 4;
+  if (!x->metrics_d) {
+    if (cudaMalloc(&x->metrics_d, sizeof(double) * 3 * (size_t)g.plane) != cudaSuccess) return PCL_ERR_OOM;
+    x->device_bytes += sizeof(double) * 3 * (size_t)g.plane;
+  }
+  const double* src[3] = {capacity, lrx, lry};
+  for (int k = 0; k < 3; ++k)  // column-major (m_xi+4) x (m_eta+4) -> rows of `pitch` doubles
+    CK(cudaMemcpy2DAsync(x->metrics_d + (size_t)k * g.plane, sizeof(double) * g.pitch, src[k], sizeof(double) * ni,
+                         sizeof(double) * ni, nj, cudaMemcpyHostToDevice, x->stream));
+  x->h2d_bytes += (long long)(3 * sizeof(double) * ni * nj);
+  CK(cudaStreamSynchronize(x->stream));  // the caller's arrays may go away on return
+  g.kap = x->metrics_d;
+  g.lrx = x->metrics_d + g.plane;
+  g.lry = x->metrics_d + 2 * g.plane;
+  g.metric = kMetricMapped;
+  drop_graph(x);
+  return PCL_OK;
+}
+
+// NORM2 of a 2-vector (face length); exact whenever one component is zero
+static double face_norm(double a, double b) {
+  if (b == 0.0) return std::fabs(a);
+  if (a == 0.0) return std::fabs(b);
+  return std::sqrt(a * a + b * b);
+}
+
+int pcl_compute_mesh_metrics(const pcl_solver_control* c, pcl_map_fn map, void* user, double* kap, double* lrx,
+                             double* lry) {
+  if (!c || !kap || !lrx || !lry || c->m_xi < 1 || c->m_eta < 1) return PCL_ERR_BADARG;
+  const double dxi = (c->xi_max - c->xi_min) / c->m_xi;      // SMOD_mesh_manipulation.f90:28
+  const double deta = (c->eta_max - c->eta_min) / c->m_eta;  // :29
+  const size_t ni = (size_t)c->m_xi + 4;
+  for (int j = -1; j <= c->m_eta + 2; ++j) {
+    for (int i = -1; i <= c->m_xi + 2; ++i) {
+      // corners 1..4 counter-clockwise, 5 = 1 (:36-47)
+      double xi[6], eta[6], x[6], y[6];
+      xi[1] = c->xi_min + (double)(i - 1) * dxi;
+      xi[2] = xi[1] + dxi;
+      xi[3] = xi[2];
+      xi[4] = xi[1];
+      xi[5] = xi[1];
+      eta[1] = c->eta_min + (double)(j - 1) * deta;
+      eta[2] = eta[1];
+      eta[3] = eta[2] + deta;
+      eta[4] = eta[3];
+      eta[5] = eta[1];
+      for (int m = 1; m <= 5; ++m) {  // finalize_mesh :137-140
+        if (map)
+          map(xi[m], eta[m], &x[m], &y[m], user);
+        else
+          x[m] = xi[m], y[m] = eta[m];
+      }
+      const size_t o = (size_t)(j + 1) * ni + (size_t)(i + 1);
+      lrx[o] = face_norm(x[4] - x[1], y[4] - y[1]) / deta;  // :147-153
+      lry[o] = face_norm(x[2] - x[1], y[2] - y[1]) / dxi;   // :156-162
+      double area = 0.0;                                     // :165-170
+      for (int m = 1; m <= 4; ++m) area = area + (0.5 * (y[m] + y[m + 1])) * (x[m] - x[m + 1]);
+      kap[o] = area / (dxi * deta);                          // :173
+    }
+  }
+  return PCL_OK;
+}
+
+int pcl_set_tile_rows(pcl_ctx* x, int rows) {
+  if (!x || rows < 4) return PCL_ERR_BADARG;
+  if (x->mixed) mixed_set_tile_rows(x->mixed, rows);
+  drop_graph(x);  // the captured launches carry the old tiling
   return PCL_OK;
 }
 

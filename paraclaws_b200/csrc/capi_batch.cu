@@ -330,7 +330,7 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   b->launches += 4;
   BCK(cudaMemcpyAsync(&h->nonunit_metric, &g.ctl->nonunit_metric, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
-  g.unit_metric = h->nonunit_metric ? 0 : 1;
+  g.metric = h->nonunit_metric ? kMetricTable : kMetricUnit;
   BCK(cudaMemcpyAsync(b->inst_d + s, &g, sizeof(GridDev), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaGetLastError());
   BCK(cudaStreamSynchronize(b->stream));

@@ -24,52 +24,53 @@ constexpr int kYT = 128;   // columns of an eta-sweep CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 16;    // rows of an eta-sweep strip
 
-template <int NT, int LIM, bool SO, bool UM>
+template <int NT, int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(NT, kXMinBlocks) xsweep_fp64_kernel(GridDev g) {
   __shared__ XSmem<NT> S;
   if (g.ctl->done) return;
-  xsweep_segment<NT, LIM, SO, UM>(g, 1 + blockIdx.y, 1 + blockIdx.x * (NT - 4), S);
+  xsweep_segment<NT, LIM, SO, MK>(g, 1 + blockIdx.y, 1 + blockIdx.x * (NT - 4), S);
 }
 
-template <int NTX, int STRIP, int LIM, bool SO, bool UM>
+template <int NTX, int STRIP, int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g) {
   if (g.ctl->done) return;
-  ysweep_strip<LIM, SO, UM>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
+  ysweep_strip<LIM, SO, MK>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
 }
 
-template <int LIM, bool SO, bool UM>
+template <int LIM, bool SO, int MK>
 void launch_x_t(const GridDev& g, cudaStream_t st) {
   dim3 gx((g.mx + (kXT - 4) - 1) / (kXT - 4), g.my);
-  xsweep_fp64_kernel<kXT, LIM, SO, UM><<<gx, kXT, 0, st>>>(g);
+  xsweep_fp64_kernel<kXT, LIM, SO, MK><<<gx, kXT, 0, st>>>(g);
 }
-template <int LIM, bool SO, bool UM>
+template <int LIM, bool SO, int MK>
 void launch_y_t(const GridDev& g, cudaStream_t st) {
   dim3 gy((g.mx + kYT - 1) / kYT, (g.my + kYS - 1) / kYS);
-  ysweep_fp64_kernel<kYT, kYS, LIM, SO, UM><<<gy, kYT, 0, st>>>(g);
+  ysweep_fp64_kernel<kYT, kYS, LIM, SO, MK><<<gy, kYT, 0, st>>>(g);
 }
-template <template <int, bool, bool> class F, bool UM>
+template <template <int, bool, int> class F, int MK>
 void dispatch_lim(const GridDev& g, cudaStream_t st) {
-  if (!g.second_order) return F<0, false, UM>::run(g, st);
+  if (!g.second_order) return F<0, false, MK>::run(g, st);
   switch (g.limiter) {
-    case 1: return F<1, true, UM>::run(g, st);
-    case 2: return F<2, true, UM>::run(g, st);
-    case 3: return F<3, true, UM>::run(g, st);
-    case 4: return F<4, true, UM>::run(g, st);
-    default: return F<0, true, UM>::run(g, st);
+    case 1: return F<1, true, MK>::run(g, st);
+    case 2: return F<2, true, MK>::run(g, st);
+    case 3: return F<3, true, MK>::run(g, st);
+    case 4: return F<4, true, MK>::run(g, st);
+    default: return F<0, true, MK>::run(g, st);
   }
 }
-template <template <int, bool, bool> class F>
+template <template <int, bool, int> class F>
 void dispatch(const GridDev& g, cudaStream_t st) {
-  if (g.unit_metric) return dispatch_lim<F, true>(g, st);
-  return dispatch_lim<F, false>(g, st);
+  if (g.metric == kMetricUnit) return dispatch_lim<F, kMetricUnit>(g, st);
+  if (g.metric == kMetricMapped) return dispatch_lim<F, kMetricMapped>(g, st);
+  return dispatch_lim<F, kMetricTable>(g, st);
 }
-template <int LIM, bool SO, bool UM>
+template <int LIM, bool SO, int MK>
 struct XL {
-  static void run(const GridDev& g, cudaStream_t st) { launch_x_t<LIM, SO, UM>(g, st); }
+  static void run(const GridDev& g, cudaStream_t st) { launch_x_t<LIM, SO, MK>(g, st); }
 };
-template <int LIM, bool SO, bool UM>
+template <int LIM, bool SO, int MK>
 struct YL {
-  static void run(const GridDev& g, cudaStream_t st) { launch_y_t<LIM, SO, UM>(g, st); }
+  static void run(const GridDev& g, cudaStream_t st) { launch_y_t<LIM, SO, MK>(g, st); }
 };
 }  // namespace
 

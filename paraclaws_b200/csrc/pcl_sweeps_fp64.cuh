@@ -2,9 +2,12 @@
 // kernels of a single grid (kernels_fp64.cu) and the persistent batched kernel
 // (batch_fp64.cu).  Include only from translation units built with --fmad=false.
 //
-// UM (unit metric): the grid's capacities and length ratios are all exactly 1.0 (checked once
-// per grid by the metric-check kernel), so x/kappa, gamma*x and the capacity mean of the
-// correction coefficient are identities and are left out; the results are the same bits.
+// MK (metric kind, pcl_types.h): kMetricTable rebuilds kappa per cell from the row/column tables
+// of the uniform grid; kMetricUnit is a uniform grid whose capacities and length ratios are all
+// exactly 1.0 (checked once per grid by the metric-check kernel), so x/kappa, gamma*x and the
+// capacity mean of the correction coefficient are identities and are left out (same bits);
+// kMetricMapped reads the per-cell capacity and face length ratios of a mapped grid
+// (MOD_solve.f90:211-233 reads length_ratio_xi(1,i,j) and (1,i+1,j) for the two faces of a cell).
 //
 // Buffer rotation replaces solution_old = solution (main.f90:201): the xi sweep reads buffer
 // cur and writes the interior rows of buffer (cur+1)%3; the eta sweep reads those rows plus the
@@ -44,8 +47,9 @@ struct XSmem {
   double red[NT / 32];
 };
 
-template <int NT, int LIM, bool SO, bool UM = false>
+template <int NT, int LIM, bool SO, int MK = kMetricTable>
 __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S) {
+  constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   const Ctl* ctl = g.ctl;
   constexpr int L = NT - 4;
   const int cur = ctl->cur, out = cur == 2 ? 0 : cur + 1;
@@ -79,7 +83,10 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
       sq[0][t] = h; sq[1][t] = hu; sq[2][t] = hv;
       sf[0][t] = F.f0; sf[1][t] = F.f1; sf[2][t] = F.f2;
       ss[t] = F.s;
-      if constexpr (!UM) sk[t] = capacity(g.rowm, g.colm, c, j, g.area_scale);
+      if constexpr (MP)
+        sk[t] = __ldg(g.kap + row + c + 1);
+      else if constexpr (!UM)
+        sk[t] = capacity(g.rowm, g.colm, c, j, g.area_scale);
     }
   }
   __syncthreads();
@@ -155,7 +162,9 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
     const int i = i0 + t;
     if (i <= mx) {
       const int c = t + 2;
-      const double gam = UM ? 1.0 : __ldg(g.rowm + (j + 1) * kRowMetrics + 2);
+      const double gam = (UM || MP) ? 1.0 : __ldg(g.rowm + (j + 1) * kRowMetrics + 2);
+      const double gl = MP ? __ldg(g.lrx + row + i + 1) : gam;  // face between cells i-1 and i
+      const double gr = MP ? __ldg(g.lrx + row + i + 2) : gam;  // face between cells i and i+1
       const double dtk = UM ? dtod : dtod / sk[c];
       const double sp = ss2[t + 1];       // A+ at interface i:   s2 * W2
       const double sm = -ss2[t + 2];      // A- at interface i+1: s1 * W1
@@ -164,7 +173,7 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
       for (int me = 0; me < 3; ++me) {
         const double ap = sp * sw2[me][t + 1];
         const double am = sm * sw1[me][t + 2];
-        double q = UM ? sq[me][c] - dtk * (ap + am) : sq[me][c] - dtk * (gam * ap + gam * am);
+        double q = UM ? sq[me][c] - dtk * (ap + am) : sq[me][c] - dtk * (gl * ap + gr * am);
         if constexpr (SO) q = q - dtk * (sft[me][t + 1] - sft[me][t]);
         o0[me * g.plane + i + 1] = q;
       }
@@ -180,6 +189,7 @@ struct YCell {
   double q[3];
   CellFlux F;
   double kap;
+  double lr;  // mapped grids: length ratio of the eta face below the cell
 };
 
 template <int LIM, bool SO, bool UM>
@@ -205,8 +215,9 @@ __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, con
   for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
 }
 
-template <int LIM, bool SO, bool UM = false>
+template <int LIM, bool SO, int MK = kMetricTable>
 __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
+  constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   Ctl* ctl = g.ctl;
   // xi-sweep validity (MOD_solve.f90:107-120), recomputed here from the reduction word
   {
@@ -229,7 +240,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
   const double* pre = buffer(g, cur);
   const double* xsw = buffer(g, xb);
   double* outp = buffer(g, yb);
-  const double gam = UM ? 1.0 : __ldg(g.colm + (ic + 1) * kColMetrics + 2);
+  const double gam = (UM || MP) ? 1.0 : __ldg(g.colm + (ic + 1) * kColMetrics + 2);
   int bad = 0;
   double smax = 0.0;
 
@@ -242,7 +253,13 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     int cb = 0;
     c.F = cell_flux<1>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
     if (jj <= my + 1) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
-    c.kap = (SO && !UM) ? capacity(g.rowm, g.colm, ic, jj, g.area_scale) : 1.0;
+    if constexpr (MP) {
+      c.kap = __ldg(g.kap + o);
+      c.lr = __ldg(g.lry + o);
+    } else {
+      c.kap = (SO && !UM) ? capacity(g.rowm, g.colm, ic, jj, g.area_scale) : 1.0;
+      c.lr = gam;
+    }
   };
   auto iface = [&](int k, const YCell& L, const YCell& R, Waves& W) -> double {
     if (k > my + 1) {
@@ -277,14 +294,15 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     load(jj + 2, cC);
     s2w = iface(jj + 2, cB, cC, W2);
     if constexpr (SO) y_corr_flux<LIM, SO, UM>(W0, W1, W2, s1, jj + 1 <= my, dtod, cA.kap, cB.kap, ft1);
-    const double kap = (SO || UM) ? cA.kap : capacity(g.rowm, g.colm, ic, jj, g.area_scale);
+    const double kap = (SO || UM || MP) ? cA.kap : capacity(g.rowm, g.colm, ic, jj, g.area_scale);
+    const double gl = MP ? cA.lr : gam, gr = MP ? cB.lr : gam;  // faces below and above the cell
     const double dtk = UM ? dtod : dtod / kap;
     const long long o = (long long)(jj + 1) * P + (ic + 1);
 #pragma unroll
     for (int me = 0; me < 3; ++me) {
       const double ap = s0 * W0.w2[me];
       const double am = (-s1) * W1.w1[me];
-      double q = UM ? cA.q[me] - dtk * (ap + am) : cA.q[me] - dtk * (gam * ap + gam * am);
+      double q = UM ? cA.q[me] - dtk * (ap + am) : cA.q[me] - dtk * (gl * ap + gr * am);
       if constexpr (SO) q = q - dtk * (ft1[me] - ft0[me]);
       if (active) outp[o + me * g.plane] = q;
     }

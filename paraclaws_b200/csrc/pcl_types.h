@@ -36,6 +36,13 @@ enum : int {
 // precision forms
 enum : int { kPrecFP64 = 0, kPrecMixed = 1 };
 
+// How the FP64 sweeps obtain the mesh metrics (capacity kappa, length ratios gamma):
+//   kMetricTable  uniform grid: kappa rebuilt per cell from the row/column tables
+//   kMetricUnit   uniform grid whose kappa and gamma are all exactly 1.0 (identities dropped)
+//   kMetricMapped mapped grid: per-cell arrays kap, lrx, lry (the reference's capacity,
+//                 length_ratio_xi(1,:,:), length_ratio_eta(1,:,:))
+enum : int { kMetricTable = 0, kMetricUnit = 1, kMetricMapped = 2 };
+
 struct StepLogEntry {   // one attempted step, as main.f90 prints it
   double dt;            // dt used by the attempt
   double cfl;           // CFL of the attempt (t_ctrl%CFL before reset_CFL)
@@ -81,8 +88,12 @@ struct GridDev {
   int mx, my, pitch;
   int bc[4];                 // xi_low, xi_high, eta_low, eta_high (1 wall, 2 zero grad., 3 const. grad.)
   int second_order, limiter; // limiter 0: unlimited correction; 1..4 by code
-  int unit_metric;           // 1: kappa(i,j) == 1 and gamma == 1 exactly on every cell the sweeps read
+  int metric;                // kMetric*
   double dxi, deta, area_scale /* d_xi*d_eta */, grav;
+  // kMetricMapped only: per-cell metrics, cell (i, j) at [(j+1)*pitch + (i+1)]
+  const double* kap;         // capacity(i, j)
+  const double* lrx;         // length ratio of the xi face between cells i-1 and i
+  const double* lry;         // length ratio of the eta face between cells j-1 and j
 };
 
 PCL_HD inline long long cell_index(int pitch, int i, int j) {

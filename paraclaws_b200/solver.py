@@ -215,6 +215,16 @@ class Solver:
         _lib.check(self.L.pcl_conservation_sums(self.h, out), "pcl_conservation_sums")
         return np.array(list(out))
 
+    def set_mesh_metrics(self, kappa: np.ndarray, lr_xi: np.ndarray, lr_eta: np.ndarray) -> None:
+        """Per-cell capacity and face length ratios of a mapped grid, shaped (m_eta+4, m_xi+4)
+        (the reference's column-major arrays); see paraclaws_b200.mesh."""
+        shape = self.shape[:2]
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (kappa, lr_xi, lr_eta)]
+        for a in arrs:
+            if a.shape != shape:
+                raise ValueError(f"metric shape {a.shape} != {shape}")
+        _lib.check(self.L.pcl_set_mesh_metrics(self.h, *(a.ctypes.data for a in arrs)), "pcl_set_mesh_metrics")
+
     def set_tile_rows(self, rows: int) -> None:
         _lib.check(self.L.pcl_set_tile_rows(self.h, int(rows)), "pcl_set_tile_rows")
 
