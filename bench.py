@@ -313,6 +313,40 @@ def form_mapped(m, steps, warmup, device, fp64_value):
             "workload": f"{m}^2 bumps (seed 0), minmod, mapping x = xi + 0.1 sin(pi eta), y = eta + 0.08 xi^2"}
 
 
+def form_snapshots(device, m=1024, time_final=0.05, snapshots=5):
+    """writeData through the device loop: a 1024^2 dam break to t = 0.05 with 5 snapshot times,
+    plain device loop vs the loop that pauses at each snapshot and formats the files on a host
+    thread while the next stretch runs."""
+    import shutil
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200.solver import Solver, run_device_loop_with_snapshots
+    c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=time_final)
+    c.number_of_snapshots = snapshots
+    out = {}
+    for mode in ("plain", "snapshots"):
+        s = Solver(c, device=device)
+        s.initial_condition()
+        s.update_rank_boundaries()
+        d = tempfile.mkdtemp(prefix="pcl_snap_")
+        t0 = time.perf_counter()
+        if mode == "plain":
+            st = s.advance()
+            n = 0
+        else:
+            times = run_device_loop_with_snapshots(s, d)
+            st = s.stats()
+            n = len(times)
+        wall = time.perf_counter() - t0
+        size = sum(os.path.getsize(os.path.join(r, f)) for r, _, fs in os.walk(d) for f in fs)
+        shutil.rmtree(d, ignore_errors=True)
+        s.close()
+        out[mode] = {"wall_s": wall, "accepted": st.accepted, "snapshots_written": n, "bytes_written": size}
+    out["formatted_mb_per_s"] = out["snapshots"]["bytes_written"] / 1e6 / max(out["snapshots"]["wall_s"], 1e-9)
+    out["workload"] = f"{m}^2 dam break to t = {time_final}, {snapshots} snapshot times plus t0, qout.dat and aout.dat"
+    return out
+
+
 def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 300, 400, 500, 700, 1000)):
     """Precision-form accuracy on the 8192^2 seeded dam break, 1000 accepted steps: the mixed
     form against FP64 at checkpoints, beside the conditioning floor of the step itself -- FP64
@@ -610,6 +644,7 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_forms:
         line["forms"] = {"mixed": form_mixed(m, args.steps, args.warmup, local, value),
                          "mapped": form_mapped(m, min(args.steps, 200), args.warmup, local, value),
+                         "snapshots": form_snapshots(local),
                          "batch": form_batch(local),
                          "serving": form_serving(local),
                          "precision": form_precision(local)}

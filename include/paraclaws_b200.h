@@ -29,7 +29,7 @@ extern "C" {
 #define PCL_ERR_BADARG (-5)     /* invalid settings or arguments */
 #define PCL_ERR_CUDA (-6)       /* CUDA runtime error */
 #define PCL_ERR_FATAL_DT (-7)   /* end_program in updateTime (time_control/MOD_time_control.f90:213-231) */
-#define PCL_ERR_IO (-8)         /* control.in / custom.in unreadable */
+#define PCL_ERR_IO (-8)         /* control.in / custom.in unreadable, or a snapshot file unwritable */
 #define PCL_ERR_FULL (-9)       /* batch: no free slot or over the memory budget */
 
 /* precision forms (custom.in) */
@@ -106,6 +106,27 @@ int pcl_download_state(pcl_ctx* ctx, double* vars);
    sqrt(x^2 + y^2) < dam_radius at the cell centre (shifted by dam_x0, dam_y0), else dam_h_out,
    hu = hv = 0, on the whole padded block.  Needs initial_condition = 1. */
 int pcl_initial_condition(pcl_ctx* ctx);
+
+/* ---- snapshots (main.f90:178 and :256-268, writeData of utility/MOD_IO.f90:397-460) ---- */
+
+/* The device-resident loop of pcl_advance, stopped after the accepted attempt whose time reaches
+   the next snapshot time (main.f90:256-258), with that step's ghost fill done: the state is what
+   the reference passes to writeData.  Returns at time_final, the accepted-step cap or an error as
+   pcl_advance does; stats->snapshot_index tells which snapshot was reached. */
+int pcl_advance_to_snapshot(pcl_ctx* ctx, pcl_run_stats* stats);
+
+/* writeData for the current state: <output_dir>/<time as F20.10, left-adjusted>/rank_0/qout.dat
+   with one record per cell of the padded block (j outer, i inner) holding h, hu, hv in the
+   reference's format(50e26.16), and aout.dat with num_aux zeros per cell (the shallow-water
+   module never sets its aux fields).  The state is transposed on the device and copied
+   asynchronously into a pinned buffer; a host thread then formats and writes the files while
+   the caller may go on stepping.  wait != 0 returns after the files are written; otherwise
+   pcl_snapshot_wait (or the next pcl_write_snapshot, or pcl_destroy) joins the writer. */
+int pcl_write_snapshot(pcl_ctx* ctx, const char* output_dir, int wait);
+int pcl_snapshot_wait(pcl_ctx* ctx);
+
+/* One value in the E26.16 field of that format, NUL-terminated (out holds 27 chars). */
+int pcl_format_e26_16(double value, char* out);
 
 /* ---- mapped (curvilinear) grids ---- */
 

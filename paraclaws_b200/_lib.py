@@ -101,6 +101,10 @@ def load(build_if_missing: bool = True):
         getattr(L, name).argtypes = [vp]
     L.pcl_solve_dimensional_split.argtypes = [vp, P(C.c_int)]
     L.pcl_set_mesh_metrics.argtypes = [vp, vp, vp, vp]
+    L.pcl_advance_to_snapshot.argtypes = [vp, P(RunStats)]
+    L.pcl_write_snapshot.argtypes = [vp, C.c_char_p, C.c_int]
+    L.pcl_snapshot_wait.argtypes = [vp]
+    L.pcl_format_e26_16.argtypes = [C.c_double, C.c_char_p]
     L.pcl_compute_mesh_metrics.argtypes = [P(SolverControl), vp, vp, vp, vp, vp]
     L.pcl_update_time.argtypes = [vp, C.c_int]
     L.pcl_set_dt.argtypes = [vp, C.c_double]

@@ -3,7 +3,13 @@
 // is built without contraction (-ffp-contract=off) to round as the reference does.
 #include <cuda_runtime.h>
 
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cerrno>
 #include <cmath>
+#include <string>
+#include <thread>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -38,6 +44,11 @@ struct pcl_ctx {
   long long launches = 0;        // kernels launched by this context
   long long graph_launches = 0;  // kernels in one launch of the captured graph
   long long h2d_bytes = 0, d2h_bytes = 0;  // bytes copied across the host boundary
+  // snapshot writer: pinned copy of the state, the copy's event, and the formatting thread
+  double* snap_h = nullptr;
+  cudaEvent_t snap_ev = nullptr;
+  std::thread snap_thread;
+  int snap_status = 0;
 };
 
 #define CK(call)                                       \
@@ -71,7 +82,7 @@ const char* pcl_status_string(int s) {
     case PCL_ERR_BADARG: return "invalid argument";
     case PCL_ERR_CUDA: return "CUDA error";
     case PCL_ERR_FATAL_DT: return "time step control cannot continue (constant dt violated)";
-    case PCL_ERR_IO: return "cannot read control file";
+    case PCL_ERR_IO: return "cannot read a control file or write a snapshot file";
     case PCL_ERR_FULL: return "batch is full or over its memory budget";
     default: return "unknown status";
   }
@@ -280,6 +291,9 @@ void init_ctl(const pcl_solver_control* c, Ctl& t) {
 
 static void free_ctx(pcl_ctx* x) {
   if (!x) return;
+  if (x->snap_thread.joinable()) x->snap_thread.join();
+  if (x->snap_ev) cudaEventDestroy(x->snap_ev);
+  if (x->snap_h) cudaFreeHost(x->snap_h);
   if (x->graph) cudaGraphExecDestroy(x->graph);
   if (x->mixed) mixed_free(x->mixed);
   cudaFree(x->bufs_d);
@@ -573,7 +587,25 @@ static int build_graph(pcl_ctx* x, int chunk) {
   return PCL_OK;
 }
 
-int pcl_advance(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats) {
+static int advance_loop(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats);
+
+int pcl_advance(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats) { return advance_loop(x, max_attempts, stats); }
+
+int pcl_advance_to_snapshot(pcl_ctx* x, pcl_run_stats* stats) {
+  if (!x) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  int r = timeop(x, kOpSetPause, 1, 0.0);
+  if (r != PCL_OK) return r;
+  const int rc = advance_loop(x, 0, nullptr);
+  r = timeop(x, kOpSetPause, 0, 0.0);  // the context steps normally again
+  if (r != PCL_OK) return r;
+  r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  if (stats) fill_stats(*x->ctl_h, x->launches, stats);
+  return rc;
+}
+
+static int advance_loop(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats) {
   if (!x) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   const int chunk = 32;
@@ -800,3 +832,123 @@ int pcl_host_free(void* p) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// snapshot writer (utility/MOD_IO.f90:397-460, writeData)
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// One value in Fortran's E26.16 edit descriptor: right-justified "[-]0.<16 digits>E+ee" (the
+// exponent letter is dropped for |exponent| > 99, as Fortran does), from the correctly rounded
+// 16 significant digits that printf's %.15e gives.
+void put_e26_16(double v, char* out) {
+  char buf[40], field[32];
+  int n;
+  if (std::isnan(v)) {
+    n = std::snprintf(field, sizeof field, "NaN");
+  } else if (std::isinf(v)) {
+    n = std::snprintf(field, sizeof field, "%s", v < 0 ? "-Infinity" : "Infinity");
+  } else {
+    std::snprintf(buf, sizeof buf, "%.15e", v);  // [-]d.ddddddddddddddde[+-]XX[X]
+    const char* p = buf;
+    const bool neg = *p == '-';
+    if (neg) ++p;
+    char digits[17];
+    digits[0] = p[0];
+    std::memcpy(digits + 1, p + 2, 15);
+    digits[16] = 0;
+    const char* e = std::strchr(p, 'e');
+    int ex = std::atoi(e + 1) + 1;
+    if (v == 0.0) ex = 0;
+    const int ax = ex < 0 ? -ex : ex;
+    if (ax <= 99)
+      n = std::snprintf(field, sizeof field, "%s0.%sE%c%02d", neg ? "-" : "", digits, ex < 0 ? '-' : '+', ax);
+    else
+      n = std::snprintf(field, sizeof field, "%s0.%s%c%03d", neg ? "-" : "", digits, ex < 0 ? '-' : '+', ax);
+  }
+  std::memset(out, ' ', 26);
+  std::memcpy(out + 26 - n, field, (size_t)n);
+}
+
+bool make_dir(const std::string& d) { return ::mkdir(d.c_str(), 0755) == 0 || errno == EEXIST; }
+
+// Format `cells` records of `per` values (3 for qout, num_aux zeros for aout when q is null) in
+// parallel row blocks and write them in order.
+bool write_records(const std::string& path, const double* q, long long cells, int per) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) return false;
+  const size_t line = (size_t)per * 26 + 1;
+  const int nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const long long block = 1LL << 16;  // records per thread and round
+  std::vector<std::string> parts(nt);
+  bool ok = true;
+  for (long long base = 0; base < cells && ok; base += block * nt) {
+    std::vector<std::thread> ts;
+    for (int t = 0; t < nt; ++t) {
+      ts.emplace_back([&, t] {
+        const long long a = base + (long long)t * block, b = std::min(cells, a + block);
+        std::string& s = parts[t];
+        s.assign(a < b ? (size_t)(b - a) * line : 0, ' ');
+        for (long long c = a; c < b; ++c) {
+          char* o = &s[(size_t)(c - a) * line];
+          for (int k = 0; k < per; ++k) put_e26_16(q ? q[c * per + k] : 0.0, o + 26 * k);
+          o[line - 1] = '\n';
+        }
+      });
+    }
+    for (auto& th : ts) th.join();
+    for (int t = 0; t < nt && ok; ++t) ok = std::fwrite(parts[t].data(), 1, parts[t].size(), f) == parts[t].size();
+  }
+  return std::fclose(f) == 0 && ok;
+}
+
+}  // namespace
+
+int pcl_write_snapshot(pcl_ctx* x, const char* output_dir, int wait) {
+  if (!x || !output_dir) return PCL_ERR_BADARG;
+  CK(cudaSetDevice(x->device));
+  if (x->snap_thread.joinable()) x->snap_thread.join();  // the previous snapshot owns the buffer
+  const long long n = pcl_state_doubles(x);
+  if (!x->snap_h && cudaMallocHost(&x->snap_h, sizeof(double) * (size_t)n) != cudaSuccess) return PCL_ERR_OOM;
+  if (!x->snap_ev && cudaEventCreateWithFlags(&x->snap_ev, cudaEventDisableTiming) != cudaSuccess) return PCL_ERR_CUDA;
+  int r = read_ctl(x);
+  if (r != PCL_OK) return r;
+  const double time = x->ctl_h->time;
+  launch_download(x->g, x->staging_d, x->stream);
+  r = check_launch(x);
+  if (r != PCL_OK) return r;
+  CK(cudaMemcpyAsync(x->snap_h, x->staging_d, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaEventRecord(x->snap_ev, x->stream));
+  x->d2h_bytes += (long long)sizeof(double) * n;
+  // output/<time F20.10, left-adjusted>/rank_0/{qout,aout}.dat (MOD_IO.f90:420-438)
+  char ts[64];
+  std::snprintf(ts, sizeof ts, "%.10f", time);
+  const std::string dir = std::string(output_dir) + "/" + ts;
+  const std::string sub = dir + "/rank_0";
+  const long long cells = (long long)(x->cfg.m_xi + 4) * (x->cfg.m_eta + 4);
+  const int naux = x->cfg.num_aux;
+  x->snap_status = PCL_OK;
+  x->snap_thread = std::thread([x, dir, sub, cells, naux] {
+    int st = PCL_OK;
+    if (cudaEventSynchronize(x->snap_ev) != cudaSuccess) st = PCL_ERR_CUDA;
+    if (st == PCL_OK && !(make_dir(dir) && make_dir(sub))) st = PCL_ERR_IO;
+    if (st == PCL_OK && !write_records(sub + "/qout.dat", x->snap_h, cells, 3)) st = PCL_ERR_IO;
+    // the SWE never sets its aux fields: num_aux zeros per cell
+    if (st == PCL_OK && !write_records(sub + "/aout.dat", nullptr, cells, naux)) st = PCL_ERR_IO;
+    x->snap_status = st;
+  });
+  return wait ? pcl_snapshot_wait(x) : PCL_OK;
+}
+
+int pcl_snapshot_wait(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  if (x->snap_thread.joinable()) x->snap_thread.join();
+  return x->snap_status;
+}
+
+int pcl_format_e26_16(double v, char* out) {
+  if (!out) return PCL_ERR_BADARG;
+  put_e26_16(v, out);
+  out[26] = 0;
+  return PCL_OK;
+}

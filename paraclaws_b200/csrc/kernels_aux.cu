@@ -47,6 +47,11 @@ __global__ void timectl_kernel(GridDev g, int op, int arg, double value) {
     case kOpFullStep:
       full_step(c, g);
       break;
+    case kOpSetPause:
+      c->pause_on_snapshot = arg;
+      c->paused = 0;
+      refresh_done(c);
+      break;
     default:
       break;
   }

@@ -15,6 +15,7 @@ enum TimeOp : int {
   kOpAdvanceSnapshot = 4, // advance_snapshot_index
   kOpFullStep = 5,        // finalize + the main-loop branch of main.f90:210-275
   kOpSetDt = 6,           // dt = value (host override, e.g. to force a rejection)
+  kOpSetPause = 7,        // pause_on_snapshot = arg, paused = 0
 };
 
 void launch_sweeps_fp64(const GridDev& g, cudaStream_t st);

@@ -92,7 +92,7 @@ __device__ __forceinline__ void reset_cfl(Ctl* c) {
 
 __device__ __forceinline__ void refresh_done(Ctl* c) {
   c->done = (c->time >= c->time_final) || (c->max_accepted > 0 && c->accepted >= c->max_accepted) ||
-            (__ldcg(&c->status) != 0);
+            (__ldcg(&c->status) != 0) || c->paused;
 }
 
 // Everything main.f90:210-275 does after the sweeps of one attempt: accept/reject, updateTime,
@@ -113,7 +113,10 @@ __device__ __forceinline__ void full_step(Ctl* c, const GridDev& g) {
   } else {
     // integrate_source_term: phi = 0 leaves finite q unchanged (MOD_solve.f90:295-336)
     ok = update_time(c, true);
-    if (ok && c->time >= next_snapshot(c) && c->snapshot_index <= c->n_snapshots) c->snapshot_index += 1;
+    if (ok && c->time >= next_snapshot(c) && c->snapshot_index <= c->n_snapshots) {
+      c->snapshot_index += 1;
+      if (c->pause_on_snapshot) c->paused = 1;  // main.f90:256-268 writes the snapshot here
+    }
     reset_cfl(c);
     c->accepted += 1;
   }

@@ -71,6 +71,8 @@ struct Ctl {
   int done;                  // time >= time_final, accepted-step cap reached, or error
   int status;                // kStatus* bits
   int nonunit_metric;        // set by the metric check when some kappa or gamma is not exactly 1
+  int pause_on_snapshot;     // pcl_advance_to_snapshot: stop after the attempt that reaches a snapshot
+  int paused;                // set then; counts as done until the host clears it
   long long attempts, accepted, max_accepted;
   long long log_cap, log_len;
   StepLogEntry* log;         // optional device log (may be null)

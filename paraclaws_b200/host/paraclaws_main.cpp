@@ -8,6 +8,10 @@
 //
 // Output: output/final_state.bin (the padded state in the reference layout, raw float64) and
 // output/steps.csv (dt used, CFL, time, next dt, ierr, snapshot index per attempted step).
+// With --snapshots also writeData's files at t0 and at every snapshot time
+// (output/<time>/rank_0/qout.dat and aout.dat, utility/MOD_IO.f90:397-460); in the device loop
+// the run pauses at each snapshot time (pcl_advance_to_snapshot) and the files are formatted
+// while the next stretch runs.
 #include <sys/stat.h>
 
 #include <cmath>
@@ -42,10 +46,11 @@ static void dam_break_ic(const pcl_solver_control& c, std::vector<double>& q) {
 }
 
 int main(int argc, char** argv) {
-  bool device_loop = false;
+  bool device_loop = false, snapshots = false;
   int device = 0;
   for (int a = 1; a < argc; ++a) {
     if (!std::strcmp(argv[a], "--device-loop")) device_loop = true;
+    else if (!std::strcmp(argv[a], "--snapshots")) snapshots = true;
     else if (!std::strcmp(argv[a], "--device") && a + 1 < argc) device = std::atoi(argv[++a]);
   }
   pcl_solver_control c;
@@ -75,9 +80,23 @@ int main(int argc, char** argv) {
   std::printf("paraCLAWs - time: %10.8f current dt: %10.8f CFL(max)=%10.5f next dt: %10.8f => snapshot: %4d\n",
               time, c.dt_initial, 0.0, c.dt_initial, 0);
   long long accepted = 0;
+  if (snapshots && (rc = pcl_write_snapshot(ctx, "output", 0))) return fail("write_snapshot", rc);  // main.f90:178
   if (device_loop) {
     pcl_run_stats st;
-    if ((rc = pcl_advance(ctx, 0, &st))) return fail("advance", rc);
+    if (snapshots) {
+      for (;;) {
+        if ((rc = pcl_advance_to_snapshot(ctx, &st))) return fail("advance_to_snapshot", rc);
+        const bool end = st.done || st.time >= c.t_final;
+        if (st.time >= c.t_final || !end) {
+          std::printf("paraCLAWs - time: %10.8f current dt: %10.8f CFL(max)=%10.5f next dt: %10.8f => snapshot: %4d\n",
+                      st.time, st.dt_previous, st.cfl, st.dt, st.snapshot_index - 1);
+          if ((rc = pcl_write_snapshot(ctx, "output", 0))) return fail("write_snapshot", rc);
+        }
+        if (end) break;
+      }
+    } else if ((rc = pcl_advance(ctx, 0, &st))) {
+      return fail("advance", rc);
+    }
     long long n = 0;
     pcl_get_step_log(ctx, nullptr, 0, &n);
     std::vector<pcl_step_record> recs((size_t)n);
@@ -117,6 +136,7 @@ int main(int argc, char** argv) {
         if (snap <= nsnap && time >= ts) {                         // :256-268
           std::printf("paraCLAWs - time: %10.8f current dt: %10.8f CFL(max)=%10.5f next dt: %10.8f => snapshot: %4d\n",
                       time, dtp, cfl, dt, snap);
+          if (snapshots && (rc = pcl_write_snapshot(ctx, "output", 0))) return fail("write_snapshot", rc);  // :260
           pcl_advance_snapshot_index(ctx);
           snap += 1;
         } else {
@@ -130,6 +150,7 @@ int main(int argc, char** argv) {
     }
   }
   std::fclose(log);
+  if (snapshots && (rc = pcl_snapshot_wait(ctx))) return fail("snapshot_wait", rc);
   if ((rc = pcl_download_state(ctx, q.data()))) return fail("download_state", rc);
   FILE* f = std::fopen("output/final_state.bin", "wb");
   std::fwrite(q.data(), sizeof(double), q.size(), f);

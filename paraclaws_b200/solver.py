@@ -200,6 +200,19 @@ class Solver:
         _lib.check(self.L.pcl_advance(self.h, int(max_attempts), C.byref(s)), "pcl_advance")
         return Stats.from_c(s)
 
+    def advance_to_snapshot(self) -> Stats:
+        """The device loop up to the next snapshot time (or the end); see write_snapshot."""
+        s = _lib.RunStats()
+        _lib.check(self.L.pcl_advance_to_snapshot(self.h, C.byref(s)), "pcl_advance_to_snapshot")
+        return Stats.from_c(s)
+
+    def write_snapshot(self, output_dir: str, wait: bool = True) -> None:
+        """writeData of the current state under output_dir (reference text format)."""
+        _lib.check(self.L.pcl_write_snapshot(self.h, str(output_dir).encode(), int(bool(wait))), "pcl_write_snapshot")
+
+    def snapshot_wait(self) -> None:
+        _lib.check(self.L.pcl_snapshot_wait(self.h), "pcl_snapshot_wait")
+
     def stats(self) -> Stats:
         s = _lib.RunStats()
         _lib.check(self.L.pcl_get_stats(self.h, C.byref(s)), "pcl_get_stats")
@@ -259,6 +272,32 @@ class Solver:
     @property
     def device_bytes(self) -> int:
         return int(self.L.pcl_device_bytes(self.h))
+
+
+def format_e26_16(value: float) -> str:
+    """A value in the E26.16 field of the reference's snapshot format."""
+    L = _lib.load()
+    buf = C.create_string_buffer(27)
+    _lib.check(L.pcl_format_e26_16(float(value), buf), "pcl_format_e26_16")
+    return buf.value.decode()
+
+
+def run_device_loop_with_snapshots(s: Solver, output_dir: str) -> list:
+    """main.f90:178-283 on the device with writeData at t0 and at every snapshot time; the
+    formatting of one snapshot overlaps the steps to the next.  Returns the snapshot times."""
+    times = [s.time]
+    s.write_snapshot(output_dir, wait=False)
+    while True:
+        st = s.advance_to_snapshot()
+        if st.time >= s.control.time_final or st.done or st.status != 0:
+            if st.status == 0 and st.time >= s.control.time_final:
+                s.write_snapshot(output_dir, wait=False)
+                times.append(st.time)
+            break
+        s.write_snapshot(output_dir, wait=False)
+        times.append(st.time)
+    s.snapshot_wait()
+    return times
 
 
 def run_host_loop(s: Solver, max_attempts: int = 0) -> StepLog:

@@ -70,3 +70,26 @@ def test_status_strings(pcl):
         s = pcl.pcl_status_string(code).decode()
         assert s and s != "unknown status"
     assert pcl.pcl_status_string(-99).decode() == "unknown status"
+
+
+def test_fortran_e26_16_field(pcl):
+    """The snapshot format's E26.16 field (utility/MOD_IO.f90:441, format(50e26.16)):
+    right-justified 0.<16 digits>E+ee, the exponent letter dropped beyond two digits."""
+    from paraclaws_b200.solver import format_e26_16
+    cases = {
+        2.0: "   0.2000000000000000E+01",
+        1.0: "   0.1000000000000000E+01",
+        0.0: "   0.0000000000000000E+00",
+        -1.5e-5: "  -0.1500000000000000E-04",
+        9.8100004196166992: "   0.9810000419616699E+01",
+        0.1: "   0.1000000000000000E+00",
+        123456.789: "   0.1234567890000000E+06",
+        1e-100: "   0.1000000000000000E-99",     # 0.1 x 10^-99: still two digits
+        1e-101: "   0.1000000000000000-100",
+        -2.5e120: "  -0.2500000000000000+121",
+        0.9999999999999999: "   0.9999999999999999E+00",
+        0.3: "   0.3000000000000000E+00",    # 0.29999999999999998889...: rounds up at 16 digits
+    }
+    for v, want in cases.items():
+        got = format_e26_16(v)
+        assert len(got) == 26 and got == " " + want, (v, got, want)

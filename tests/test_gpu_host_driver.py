@@ -34,3 +34,26 @@ def test_host_program_matches_oracle(pcl, oracle_lib, tmp_path, device_loop):
     assert np.array_equal(np.atleast_1d(steps["dt"]), log.dt)
     assert np.array_equal(np.atleast_1d(steps["ierr"]).astype(int), log.ierr)
     assert np.array_equal(q, o.state())
+
+
+def test_host_program_snapshots_same_in_both_loops(pcl, tmp_path):
+    """--snapshots writes writeData's files at t0 and every snapshot time; the host-driven loop
+    and the device loop (paused at snapshot times) write identical files."""
+    c = ctl.dam_break_control(28, limiter=1, bc=3, time_final=0.04)
+    c.number_of_snapshots = 4
+    exe = B.HOST_BIN if B.HOST_BIN.exists() else B.build_host_driver()
+    trees = []
+    for mode in ([], ["--device-loop"]):
+        d = tmp_path / ("dev" if mode else "host")
+        d.mkdir()
+        ctl.write_control(d / "control.in", c)
+        ctl.write_custom(d / "custom.in", ctl.CustomSettings())
+        r = subprocess.run([str(exe), "--snapshots"] + mode, cwd=d, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        snaps = sorted((p for p in (d / "output").iterdir() if p.is_dir()), key=lambda p: float(p.name))
+        trees.append({p.name: ((p / "rank_0" / "qout.dat").read_text(), (p / "rank_0" / "aout.dat").read_text())
+                      for p in snaps})
+    assert list(trees[0]) == ["%.10f" % t for t in (0.0, 0.01, 0.02, 0.03, 0.04)]
+    assert trees[0] == trees[1]
+    body = trees[0]["0.0400000000"][0].splitlines()
+    assert len(body) == 32 * 32 and all(len(line) == 78 for line in body)
