@@ -31,6 +31,7 @@ extern "C" {
 #define PCL_ERR_FATAL_DT (-7)   /* end_program in updateTime (time_control/MOD_time_control.f90:213-231) */
 #define PCL_ERR_IO (-8)         /* control.in / custom.in unreadable, or a snapshot file unwritable */
 #define PCL_ERR_FULL (-9)       /* batch: no free slot or over the memory budget */
+#define PCL_ERR_USER (-10)      /* the user boundary hook returned an error */
 
 /* precision forms (custom.in) */
 #define PCL_PREC_FP64 0   /* bit-compatible FP64 path (the drop-in) */
@@ -127,6 +128,35 @@ int pcl_snapshot_wait(pcl_ctx* ctx);
 
 /* One value in the E26.16 field of that format, NUL-terminated (out holds 27 chars). */
 int pcl_format_e26_16(double value, char* out);
+
+/* ---- user boundary condition (code 1, BC_USER of SMOD_boundary_conditions.f90:13) ---- */
+
+/* What a user boundary hook sees: the context's device state and the current-buffer index. */
+typedef struct pcl_bc_view {
+  double* state;               /* device: rotation buffer b, plane p (0 h, 1 hu, 2 hv) at
+                                  state + b*buffer_stride + p*plane_stride */
+  long long buffer_stride;     /* doubles */
+  long long plane_stride;      /* doubles */
+  int pitch;                   /* doubles per row: cell (i, j), i, j = -1 .. m+2, at (j+1)*pitch + (i+1) */
+  int m_xi, m_eta;
+  int centre_stride;           /* centre of column i at xi_centre[(i+1)*centre_stride], row j likewise */
+  const double* xi_centre;     /* device */
+  const double* eta_centre;    /* device */
+  const int* current_buffer;   /* device int: index of the buffer holding the current solution */
+  const int* attempt_accepted; /* device int: 1 when the attempt just taken was accepted */
+} pcl_bc_view;
+
+/* The reference leaves BC_USER unimplemented (it aborts, SMOD_boundary_conditions.f90:83-211);
+   this build fills it with a reflective wall unless a hook is set.  The hook enqueues the
+   caller's own device work on `stream` (a cudaStream_t) for the sides in `sides` (bit 0 xi low,
+   1 xi high, 2 eta low, 3 eta high: those coded 1) and returns 0, or nonzero on failure
+   (PCL_ERR_USER).  It must only enqueue: the library calls it wherever it fills ghosts, also
+   while capturing the CUDA graphs of pcl_advance, where the fill of every attempt is in the
+   graph and must do nothing on the device unless *attempt_accepted == 1.  force = 1 marks a
+   fill that always runs (pcl_update_rank_boundaries).  The current buffer changes every
+   accepted step, so device code reads *current_buffer.  Corner ghosts are never read. */
+typedef int (*pcl_user_bc_fn)(const pcl_bc_view* view, int sides, int force, void* stream, void* user);
+int pcl_set_user_bc(pcl_ctx* ctx, pcl_user_bc_fn fn, void* user);
 
 /* ---- mapped (curvilinear) grids ---- */
 

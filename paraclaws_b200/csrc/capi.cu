@@ -45,6 +45,9 @@ struct pcl_ctx {
   long long graph_launches = 0;  // kernels in one launch of the captured graph
   long long h2d_bytes = 0, d2h_bytes = 0;  // bytes copied across the host boundary
   // snapshot writer: pinned copy of the state, the copy's event, and the formatting thread
+  pcl_user_bc_fn user_bc = nullptr;  // hook for sides coded 1
+  void* user_bc_data = nullptr;
+  int user_bc_rc = 0;                 // first failure of the hook since the last check
   double* snap_h = nullptr;
   cudaEvent_t snap_ev = nullptr;
   std::thread snap_thread;
@@ -84,6 +87,7 @@ const char* pcl_status_string(int s) {
     case PCL_ERR_FATAL_DT: return "time step control cannot continue (constant dt violated)";
     case PCL_ERR_IO: return "cannot read a control file or write a snapshot file";
     case PCL_ERR_FULL: return "batch is full or over its memory budget";
+    case PCL_ERR_USER: return "the user boundary hook failed";
     default: return "unknown status";
   }
 }
@@ -456,12 +460,57 @@ int pcl_download_state(pcl_ctx* x, double* vars) {
   return PCL_OK;
 }
 
+// The ghost fill: the built-in kernel for every side, then the user hook for sides coded 1.
+static void enqueue_ghost(pcl_ctx* x, int force) {
+  launch_ghost(x->g, force, x->stream);
+  if (!x->user_bc) return;
+  int sides = 0;
+  for (int s = 0; s < 4; ++s)
+    if (x->g.bc[s] == 1) sides |= 1 << s;
+  if (!sides) return;
+  pcl_bc_view v;
+  v.state = x->g.state;
+  v.buffer_stride = x->g.bufstride;
+  v.plane_stride = x->g.plane;
+  v.pitch = x->g.pitch;
+  v.m_xi = x->g.mx;
+  v.m_eta = x->g.my;
+  v.centre_stride = kColMetrics;
+  v.xi_centre = x->g.colm + 3;
+  v.eta_centre = x->g.rowm + 3;
+  v.current_buffer = &x->ctl_d->cur;
+  v.attempt_accepted = &x->ctl_d->ierr;
+  const int rc = x->user_bc(&v, sides, force, (void*)x->stream, x->user_bc_data);
+  if (rc != 0 && x->user_bc_rc == 0) x->user_bc_rc = PCL_ERR_USER;
+}
+
+static int take_user_bc_rc(pcl_ctx* x) {
+  const int r = x->user_bc_rc;
+  x->user_bc_rc = 0;
+  return r;
+}
+
 int pcl_update_rank_boundaries(pcl_ctx* x) {
   if (!x) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
-  launch_ghost(x->g, 1, x->stream);
+  enqueue_ghost(x, 1);
   x->launches += 1;
+  const int r = take_user_bc_rc(x);
+  if (r != PCL_OK) return r;
   return check_launch(x);
+}
+
+int pcl_set_user_bc(pcl_ctx* x, pcl_user_bc_fn fn, void* user) {
+  if (!x) return PCL_ERR_BADARG;
+  x->user_bc = fn;
+  x->user_bc_data = user;
+  x->g.user_bc = fn ? 1 : 0;
+  if (x->graph) {  // the captured graphs hold the previous fill
+    cudaGraphExecDestroy(x->graph);
+    x->graph = nullptr;
+    x->graph_chunk = 0;
+  }
+  return PCL_OK;
 }
 
 static int sweep_kernels(const pcl_ctx* x) { return x->cfg.precision_mode == PCL_PREC_MIXED ? 1 : 2; }
@@ -563,7 +612,7 @@ int pcl_get_stats(pcl_ctx* x, pcl_run_stats* s) {
 static void enqueue_attempt(pcl_ctx* x) {
   launch_sweeps(x);
   launch_timectl(x->g, kOpFullStep, 0, 0.0, x->stream);
-  launch_ghost(x->g, 0, x->stream);
+  enqueue_ghost(x, 0);
   x->launches += 2;
 }
 
@@ -580,6 +629,11 @@ static int build_graph(pcl_ctx* x, int chunk) {
   CK(cudaStreamEndCapture(x->stream, &gr));
   x->graph_launches = x->launches - before;  // kernels per graph launch
   x->launches = before;
+  const int urc = take_user_bc_rc(x);
+  if (urc != PCL_OK) {
+    cudaGraphDestroy(gr);
+    return urc;
+  }
   cudaError_t e = cudaGraphInstantiate(&x->graph, gr, 0);
   cudaGraphDestroy(gr);
   if (e != cudaSuccess) return PCL_ERR_CUDA;
@@ -622,6 +676,8 @@ static int advance_loop(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats
     if (max_attempts > 0 && doneatt >= max_attempts) break;
     if (max_attempts > 0 && max_attempts - doneatt < chunk) {
       for (long long k = doneatt; k < max_attempts; ++k) enqueue_attempt(x);
+      r = take_user_bc_rc(x);
+      if (r != PCL_OK) return r;
     } else {
       CK(cudaGraphLaunch(x->graph, x->stream));
       x->launches += x->graph_launches;

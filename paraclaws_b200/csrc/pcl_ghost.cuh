@@ -23,6 +23,7 @@ __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid)
   if (side >= 4) return;
   const long long P = g.pitch;
   const int bc = g.bc[side];
+  if (bc == 1 && g.user_bc) return;  // the user boundary hook fills this side
   if (side < 2) {  // xi boundaries, rows j = 1 .. m_eta
     const int j = idx;
     if (j > my) return;

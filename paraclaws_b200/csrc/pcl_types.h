@@ -91,6 +91,7 @@ struct GridDev {
   int bc[4];                 // xi_low, xi_high, eta_low, eta_high (1 wall, 2 zero grad., 3 const. grad.)
   int second_order, limiter; // limiter 0: unlimited correction; 1..4 by code
   int metric;                // kMetric*
+  int user_bc;               // 1: sides coded 1 are filled by the host's user hook, not the wall
   double dxi, deta, area_scale /* d_xi*d_eta */, grav;
   // kMetricMapped only: per-cell metrics, cell (i, j) at [(j+1)*pitch + (i+1)]
   const double* kap;         // capacity(i, j)

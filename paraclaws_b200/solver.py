@@ -200,6 +200,11 @@ class Solver:
         _lib.check(self.L.pcl_advance(self.h, int(max_attempts), C.byref(s)), "pcl_advance")
         return Stats.from_c(s)
 
+    def set_user_bc(self, fn_address: Optional[int], user: Optional[int] = None) -> None:
+        """Install a pcl_user_bc_fn (its address, e.g. from a ctypes CDLL) for sides coded 1;
+        None restores the built-in wall."""
+        _lib.check(self.L.pcl_set_user_bc(self.h, fn_address, user), "pcl_set_user_bc")
+
     def advance_to_snapshot(self) -> Stats:
         """The device loop up to the next snapshot time (or the end); see write_snapshot."""
         s = _lib.RunStats()
