@@ -131,8 +131,9 @@ int pcl_format_e26_16(double value, char* out);
 
 /* ---- user boundary condition (code 1, BC_USER of SMOD_boundary_conditions.f90:13) ---- */
 
-/* What a user boundary hook sees: the context's device state and the current-buffer index. */
-typedef struct pcl_bc_view {
+/* What a device hook (user boundary condition, source term) sees: the context's device state,
+   the current-buffer index and the attempt's flags. */
+typedef struct pcl_device_view {
   double* state;               /* device: rotation buffer b, plane p (0 h, 1 hu, 2 hv) at
                                   state + b*buffer_stride + p*plane_stride */
   long long buffer_stride;     /* doubles */
@@ -144,7 +145,9 @@ typedef struct pcl_bc_view {
   const double* eta_centre;    /* device */
   const int* current_buffer;   /* device int: index of the buffer holding the current solution */
   const int* attempt_accepted; /* device int: 1 when the attempt just taken was accepted */
-} pcl_bc_view;
+  const double* step_dt;       /* device double: dt of that attempt */
+} pcl_device_view;
+typedef pcl_device_view pcl_bc_view;
 
 /* The reference leaves BC_USER unimplemented (it aborts, SMOD_boundary_conditions.f90:83-211);
    this build fills it with a reflective wall unless a hook is set.  The hook enqueues the
@@ -157,6 +160,18 @@ typedef struct pcl_bc_view {
    accepted step, so device code reads *current_buffer.  Corner ghosts are never read. */
 typedef int (*pcl_user_bc_fn)(const pcl_bc_view* view, int sides, int force, void* stream, void* user);
 int pcl_set_user_bc(pcl_ctx* ctx, pcl_user_bc_fn fn, void* user);
+
+/* ---- source term (integrate_source_term, solver/MOD_solve.f90:295-336) ---- */
+
+/* The reference integrates a user source_function phi by forward Euler, q_p += phi_p * dt, on
+   the interior cells after an accepted attempt and before the ghost fill (main.f90:238).  The
+   dam break's phi is 0, a no-op the library skips.  A source hook enqueues the caller's own
+   kernel doing that update on `stream`; `*step_dt` on the device is the attempt's dt.  The hook
+   runs from pcl_integrate_source_term (force = 1) and inside the device loop's graphs after
+   every attempt's time control (force = 0: do nothing on the device unless
+   *attempt_accepted == 1).  Returns 0, or nonzero on failure (PCL_ERR_USER). */
+typedef int (*pcl_source_fn)(const pcl_device_view* view, int force, void* stream, void* user);
+int pcl_set_source_hook(pcl_ctx* ctx, pcl_source_fn fn, void* user);
 
 /* ---- mapped (curvilinear) grids ---- */
 

@@ -102,6 +102,7 @@ struct orc {
     double *lambda, *waves, *Am, *Ap, *f, *wn2l, *wn2r;
     tctl_t t;
     int status;
+    double friction; /* source_function phi = (0, -c hu, -c hv); 0: phi = 0 */
 };
 
 #define CID(o, i, j) ((size_t)((j) + 1) * (size_t)(o)->ni + (size_t)((i) + 1))
@@ -741,6 +742,8 @@ void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double
     if (lr_eta) memcpy(lr_eta, o->lr_eta, n);
 }
 
+void orc_set_friction(orc_t* o, double c) { o->friction = c; }
+
 void orc_set_mesh(orc_t* o, const double* kappa, const double* lr_xi, const double* lr_eta)
 {
     const size_t n = sizeof(double) * (size_t)o->ni * (size_t)o->nj;
@@ -801,7 +804,16 @@ int orc_run(orc_t* o, long long max_attempts, double* log_d, int* log_i, long lo
             memcpy(o->vars, o->vars_old, nbytes); /* :221 */
             orc_reset_cfl(o);
         } else {
-            /* integrate_source_term with phi = 0 is q + 0*dt: no change for finite q */
+            /* integrate_source_term (MOD_solve.f90:295-336): with phi = 0 it is q + 0*dt, no change
+               for finite q; with friction q_p = q_p + phi_p*dt per interior cell, j outer */
+            if (o->friction != 0.0) {
+                const double dt = o->t.dt; /* get_dt(): updateTime has not run yet */
+                for (int j = 1; j <= o->p.m_eta; ++j)
+                    for (int i = 1; i <= o->p.m_xi; ++i) {
+                        const double phi[3] = {0.0, -o->friction * Q(o, 1, i, j), -o->friction * Q(o, 2, i, j)};
+                        for (int me = 0; me < NEQ; ++me) Q(o, me, i, j) = Q(o, me, i, j) + phi[me] * dt;
+                    }
+            }
             orc_update_rank_boundaries(o);
             rc = tctl_update_time(&o->t, 1);
             if (rc == ORC_OK && o->t.time >= tctl_next_snapshot(&o->t) &&

@@ -63,6 +63,10 @@ void orc_get_state(const orc_t* o, double* vars);
 
 /* mesh metrics (same padded layout, one value per cell) */
 void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double* lr_xi, double* lr_eta);
+/* a non-zero source_function for tests of the source hook: phi = (0, -c*hu, -c*hv) (linear
+   friction), integrated by integrate_source_term (solver/MOD_solve.f90:295-336); c = 0 is the
+   dam break's phi = 0 */
+void orc_set_friction(orc_t* o, double c);
 /* replace capacity and face length ratios by those of a mapped grid (finalize_mesh of a user
    mapping, SMOD_mesh_manipulation.f90:147-173); cell centres stay computational */
 void orc_set_mesh(orc_t* o, const double* kappa, const double* lr_xi, const double* lr_eta);

@@ -67,6 +67,7 @@ def lib():
         L.orc_get_state.argtypes = [C.c_void_p, dp]
         L.orc_get_mesh.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
         L.orc_set_mesh.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_set_friction.argtypes = [C.c_void_p, C.c_double]
         L.orc_update_rank_boundaries.argtypes = [C.c_void_p]
         L.orc_solve_dimensional_split.argtypes = [C.c_void_p, P(C.c_int)]
         L.orc_sweep.argtypes = [C.c_void_p, C.c_int, P(C.c_double)]
@@ -177,6 +178,10 @@ class Oracle:
         arrs = [np.empty(n, dtype=np.float64) for _ in range(5)]
         lib().orc_get_mesh(self.h, *arrs)
         return dict(zip(["xi", "eta", "kappa", "lr_xi", "lr_eta"], arrs))
+
+    def set_friction(self, c: float) -> None:
+        """source_function phi = (0, -c hu, -c hv) (0: the dam break's phi = 0)."""
+        lib().orc_set_friction(self.h, float(c))
 
     def set_mesh(self, kappa, lr_xi, lr_eta) -> None:
         """Metrics of a mapped grid (arrays shaped like mesh()['kappa'])."""

@@ -106,6 +106,7 @@ def load(build_if_missing: bool = True):
     L.pcl_snapshot_wait.argtypes = [vp]
     L.pcl_format_e26_16.argtypes = [C.c_double, C.c_char_p]
     L.pcl_set_user_bc.argtypes = [vp, vp, vp]
+    L.pcl_set_source_hook.argtypes = [vp, vp, vp]
     L.pcl_compute_mesh_metrics.argtypes = [P(SolverControl), vp, vp, vp, vp, vp]
     L.pcl_update_time.argtypes = [vp, C.c_int]
     L.pcl_set_dt.argtypes = [vp, C.c_double]

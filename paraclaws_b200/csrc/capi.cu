@@ -47,7 +47,9 @@ struct pcl_ctx {
   // snapshot writer: pinned copy of the state, the copy's event, and the formatting thread
   pcl_user_bc_fn user_bc = nullptr;  // hook for sides coded 1
   void* user_bc_data = nullptr;
-  int user_bc_rc = 0;                 // first failure of the hook since the last check
+  pcl_source_fn source = nullptr;     // source-term hook
+  void* source_data = nullptr;
+  int user_bc_rc = 0;                 // first failure of a hook since the last check
   double* snap_h = nullptr;
   cudaEvent_t snap_ev = nullptr;
   std::thread snap_thread;
@@ -460,15 +462,7 @@ int pcl_download_state(pcl_ctx* x, double* vars) {
   return PCL_OK;
 }
 
-// The ghost fill: the built-in kernel for every side, then the user hook for sides coded 1.
-static void enqueue_ghost(pcl_ctx* x, int force) {
-  launch_ghost(x->g, force, x->stream);
-  if (!x->user_bc) return;
-  int sides = 0;
-  for (int s = 0; s < 4; ++s)
-    if (x->g.bc[s] == 1) sides |= 1 << s;
-  if (!sides) return;
-  pcl_bc_view v;
+static void fill_view(const pcl_ctx* x, pcl_device_view& v) {
   v.state = x->g.state;
   v.buffer_stride = x->g.bufstride;
   v.plane_stride = x->g.plane;
@@ -480,8 +474,42 @@ static void enqueue_ghost(pcl_ctx* x, int force) {
   v.eta_centre = x->g.rowm + 3;
   v.current_buffer = &x->ctl_d->cur;
   v.attempt_accepted = &x->ctl_d->ierr;
+  v.step_dt = &x->ctl_d->dt_step;
+}
+
+// The ghost fill: the built-in kernel for every side, then the user hook for sides coded 1.
+static void enqueue_ghost(pcl_ctx* x, int force) {
+  launch_ghost(x->g, force, x->stream);
+  if (!x->user_bc) return;
+  int sides = 0;
+  for (int s = 0; s < 4; ++s)
+    if (x->g.bc[s] == 1) sides |= 1 << s;
+  if (!sides) return;
+  pcl_device_view v;
+  fill_view(x, v);
   const int rc = x->user_bc(&v, sides, force, (void*)x->stream, x->user_bc_data);
   if (rc != 0 && x->user_bc_rc == 0) x->user_bc_rc = PCL_ERR_USER;
+}
+
+// integrate_source_term: nothing for phi = 0, else the source hook
+static void enqueue_source(pcl_ctx* x, int force) {
+  if (!x->source) return;
+  pcl_device_view v;
+  fill_view(x, v);
+  const int rc = x->source(&v, force, (void*)x->stream, x->source_data);
+  if (rc != 0 && x->user_bc_rc == 0) x->user_bc_rc = PCL_ERR_USER;
+}
+
+int pcl_set_source_hook(pcl_ctx* x, pcl_source_fn fn, void* user) {
+  if (!x) return PCL_ERR_BADARG;
+  x->source = fn;
+  x->source_data = user;
+  if (x->graph) {  // the captured graphs hold the previous step
+    cudaGraphExecDestroy(x->graph);
+    x->graph = nullptr;
+    x->graph_chunk = 0;
+  }
+  return PCL_OK;
 }
 
 static int take_user_bc_rc(pcl_ctx* x) {
@@ -538,7 +566,15 @@ int pcl_solve_dimensional_split(pcl_ctx* x, int* ierr) {
 }
 
 int pcl_restore_solution(pcl_ctx* x) { return x ? PCL_OK : PCL_ERR_BADARG; }
-int pcl_integrate_source_term(pcl_ctx* x) { return x ? PCL_OK : PCL_ERR_BADARG; }
+int pcl_integrate_source_term(pcl_ctx* x) {
+  if (!x) return PCL_ERR_BADARG;
+  if (!x->source) return PCL_OK;  // phi = 0: q + 0*dt leaves every finite q unchanged
+  CK(cudaSetDevice(x->device));
+  enqueue_source(x, 1);
+  const int r = take_user_bc_rc(x);
+  if (r != PCL_OK) return r;
+  return check_launch(x);
+}
 
 static int timeop(pcl_ctx* x, int op, int arg, double value) {
   if (!x) return PCL_ERR_BADARG;
@@ -612,6 +648,7 @@ int pcl_get_stats(pcl_ctx* x, pcl_run_stats* s) {
 static void enqueue_attempt(pcl_ctx* x) {
   launch_sweeps(x);
   launch_timectl(x->g, kOpFullStep, 0, 0.0, x->stream);
+  enqueue_source(x, 0);
   enqueue_ghost(x, 0);
   x->launches += 2;
 }

@@ -62,6 +62,7 @@ __device__ __forceinline__ bool update_time(Ctl* c, bool step_valid) {
 // CFL reduction result and accept/reject (MOD_solve.f90:101-174): CFL_local is the running
 // max over both sweeps and t_ctrl%CFL = max(CFL, CFL_local) after each sweep.
 __device__ __forceinline__ void finalize_solve(Ctl* c, const GridDev& g) {
+  c->dt_step = c->dt;
   // the reduction words are written by atomics from other CTAs of the same (batched) launch:
   // read them at L2, past this SM's L1
   const double sx = __longlong_as_double((long long)__ldcg(&c->smax_x));

@@ -63,6 +63,7 @@ struct Ctl {
   int adaptive, snapshot_exception;
   // ---- per attempt ----
   double dtod_x, dtod_y;     // dt/d_xi, dt/d_eta for the current dt
+  double dt_step;            // dt of the attempt being finalised (integrate_source_term's get_dt())
   unsigned long long smax_x, smax_y;  // IEEE bits of max wave speed s2 per sweep (>= 0)
   double cfl_x, cfl_y;       // CFL_local after the xi sweep / after both sweeps
   int valid_x;               // xi-sweep validity (early reject, MOD_solve.f90:107-120)

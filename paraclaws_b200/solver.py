@@ -205,6 +205,10 @@ class Solver:
         None restores the built-in wall."""
         _lib.check(self.L.pcl_set_user_bc(self.h, fn_address, user), "pcl_set_user_bc")
 
+    def set_source_hook(self, fn_address: Optional[int], user: Optional[int] = None) -> None:
+        """Install a pcl_source_fn (integrate_source_term with a non-zero phi); None: phi = 0."""
+        _lib.check(self.L.pcl_set_source_hook(self.h, fn_address, user), "pcl_set_source_hook")
+
     def advance_to_snapshot(self) -> Stats:
         """The device loop up to the next snapshot time (or the end); see write_snapshot."""
         s = _lib.RunStats()
