@@ -347,6 +347,41 @@ def form_snapshots(device, m=1024, time_final=0.05, snapshots=5):
     return out
 
 
+def form_equations(m, steps, warmup, device, fp64_value):
+    """The generic equation-module path on the plain-large grid: the dam-break Jacobian through it
+    (same results as the specialised kernels) and linear acoustics from a pressure pulse."""
+    import numpy as np
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200 import ic
+    from paraclaws_b200.solver import Solver
+    c = workload(m)
+    out = {}
+    for name, module, prm in (("shallow_water_generic", ctl.EQ_SHALLOW_WATER_GENERIC, ()),
+                              ("acoustics", ctl.EQ_ACOUSTICS, (2.0, 0.5))):
+        if module == ctl.EQ_ACOUSTICS:
+            x, y = np.meshgrid(*ic.cell_centres(m, m))
+            q = np.zeros((m + 4, m + 4, 3))
+            q[..., 0] = np.exp(-(x ** 2 + y ** 2) / 0.01)
+        else:
+            q = ic.gaussian_bumps(m, m, seed=0)
+        s = Solver(c, ctl.CustomSettings(max_accepted_steps=steps), device=device)
+        s.set_equation(module, prm)
+        s.upload(q)
+        s.update_rank_boundaries()
+        s.advance(max_attempts=warmup)
+        s.upload(q)
+        s.update_rank_boundaries()
+        s.reset_time_control()
+        st, ms = _timed_advance(s, steps, torch)
+        s.close()
+        out[name] = {"value": st.accepted * m * m / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / max(steps, 1)}
+    out["specialised_fp64_value"] = fp64_value
+    out["workload"] = f"{m}^2, minmod, {steps} steps"
+    return out
+
+
 def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 300, 400, 500, 700, 1000)):
     """Precision-form accuracy on the 8192^2 seeded dam break, 1000 accepted steps: the mixed
     form against FP64 at checkpoints, beside the conditioning floor of the step itself -- FP64
@@ -644,6 +679,7 @@ def run_ours(args) -> None:
         line["forms"] = {"mixed": form_mixed(m, args.steps, args.warmup, local, value),
                          "mapped": form_mapped(m, min(args.steps, 200), args.warmup, local, value),
                          "snapshots": form_snapshots(local),
+                         "equations": form_equations(m, min(args.steps, 200), args.warmup, local, value),
                          "batch": form_batch(local),
                          "serving": form_serving(local),
                          "precision": form_precision(local)}

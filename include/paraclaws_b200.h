@@ -173,6 +173,23 @@ int pcl_set_user_bc(pcl_ctx* ctx, pcl_user_bc_fn fn, void* user);
 typedef int (*pcl_source_fn)(const pcl_device_view* view, int force, void* stream, void* user);
 int pcl_set_source_hook(pcl_ctx* ctx, pcl_source_fn fn, void* user);
 
+/* ---- equation modules (getJakobi interface, user_subroutines/MOD_user_subroutines.f90) ---- */
+
+/* The reference builds one equation module into the program (a USER_DIR jakobian submodule
+   replaces the example's).  This library compiles its modules in and takes one per context:
+     PCL_EQ_SHALLOW_WATER          the dam-break module (examples/2D_dam_break/cartesian/
+                                   SMOD_jakobian.f90:44-53), specialised kernels; the default
+     PCL_EQ_SHALLOW_WATER_GENERIC  the same Jacobian through the generic path
+     PCL_EQ_ACOUSTICS              linear acoustics, q = (p, u, v), params (K, rho)
+   The generic path runs the reference's step for the module's Jacobian: flux J(q).q in dgemv
+   order, HLL with the largest |eigenvalue| of both cells (closed form per module), the limiter
+   and the correction on the three components.  params: shallow water takes g (default: the
+   control's grav), acoustics K and rho (both > 0).  FP64 contexts on uniform grids only. */
+#define PCL_EQ_SHALLOW_WATER 0
+#define PCL_EQ_SHALLOW_WATER_GENERIC 1
+#define PCL_EQ_ACOUSTICS 2
+int pcl_set_equation(pcl_ctx* ctx, int module, const double* params, int nparams);
+
 /* ---- mapped (curvilinear) grids ---- */
 
 /* Mesh metrics of a mapped grid, as finalize_mesh leaves them in the reference

@@ -26,6 +26,8 @@
  *      faithful cost model of the reference and its closest runnable arithmetic.
  */
 #include "oracle.h"
+/* equation modules beyond the dam break (the caller's physics, shared with the CUDA path) */
+#include "../paraclaws_b200/csrc/pcl_equations.h"
 
 #include <dlfcn.h>
 #include <stdio.h>
@@ -103,6 +105,8 @@ struct orc {
     tctl_t t;
     int status;
     double friction; /* source_function phi = (0, -c hu, -c hv); 0: phi = 0 */
+    int eq;          /* equation module (pcl_equations.h); 0: this file's shallow water */
+    double eqp[2];
 };
 
 #define CID(o, i, j) ((size_t)((j) + 1) * (size_t)(o)->ni + (size_t)((i) + 1))
@@ -347,20 +351,41 @@ static int eigenvalues(int mode, int ixy, const double* J, const double* q, doub
 }
 
 /* HLL: solver/SMOD_approximate_Riemann_solvers.f90:15-102 for one interface */
+/* getJakobi / calculateEigenSolution of another equation module: its Jacobian, and in closed-form
+   mode its eigenvalues (mode 1 still calls dgeev on the module's Jacobian) */
+static int module_jakobi(int eq, const double* prm, int ixy, const double* q, double* J)
+{
+    return pcl_eq_jacobian(eq, ixy, q, prm, J) ? ORC_ERR_NAN : ORC_OK;
+}
+
+static int hll_core_eq(int eq, const double* prm, int ixy, const double* qL, const double* qR, double g, int mode,
+                       double* lam2, double* W);
+
 static int hll_core(int ixy, const double* qL, const double* qR, double g, int mode, double* lam2,
                     double* W /* [mw*3+me] */)
 {
+    return hll_core_eq(0, NULL, ixy, qL, qR, g, mode, lam2, W);
+}
+
+static int hll_core_eq(int eq, const double* prm, int ixy, const double* qL, const double* qR, double g, int mode,
+                       double* lam2, double* W /* [mw*3+me] */)
+{
     double JL[9], JR[9], lL[3] = {0, 0, 0}, lR[3] = {0, 0, 0}, fL[3], fR[3];
     int st = ORC_OK, s;
-    if ((s = jakobi(ixy, qL, g, JL)) != ORC_OK) st = s;
-    if ((s = jakobi(ixy, qR, g, JR)) != ORC_OK) st = s;
+    if ((s = eq ? module_jakobi(eq, prm, ixy, qL, JL) : jakobi(ixy, qL, g, JL)) != ORC_OK) st = s;
+    if ((s = eq ? module_jakobi(eq, prm, ixy, qR, JR) : jakobi(ixy, qR, g, JR)) != ORC_OK) st = s;
     if (st != ORC_OK) {
         lam2[0] = lam2[1] = 0.0;
         for (int k = 0; k < 6; ++k) W[k] = 0.0;
         return st;
     }
-    if ((s = eigenvalues(mode, ixy, JL, qL, g, lL)) != ORC_OK) st = s;
-    if ((s = eigenvalues(mode, ixy, JR, qR, g, lR)) != ORC_OK) st = s;
+    if (eq && mode == 0) {
+        if (pcl_eq_eigenvalues(eq, ixy, qL, prm, lL)) st = ORC_ERR_NEG_DEPTH;
+        if (pcl_eq_eigenvalues(eq, ixy, qR, prm, lR)) st = ORC_ERR_NEG_DEPTH;
+    } else {
+        if ((s = eigenvalues(mode, ixy, JL, qL, g, lL)) != ORC_OK) st = s;
+        if ((s = eigenvalues(mode, ixy, JR, qR, g, lR)) != ORC_OK) st = s;
+    }
     /* s2 = maxval([abs(lambda_left), abs(lambda_right)]) :190 */
     double s2 = fabs(lL[0]);
     for (int k = 1; k < 3; ++k) s2 = fabs(lL[k]) > s2 ? fabs(lL[k]) : s2;
@@ -400,7 +425,7 @@ static void wave_decomposition(orc_t* o, int ixy, int i, int j)
         qL[me] = Q(o, me, il, jl);
         qR[me] = Q(o, me, i, j);
     }
-    int st = hll_core(ixy, qL, qR, o->p.grav, o->p.eigen_mode, lam2, W);
+    int st = hll_core_eq(o->eq, o->eqp, ixy, qL, qR, o->p.grav, o->p.eigen_mode, lam2, W);
     if (st != ORC_OK) set_status(o, st);
     LAM(o, 0, i, j) = lam2[0];
     LAM(o, 1, i, j) = lam2[1];
@@ -743,6 +768,15 @@ void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double
 }
 
 void orc_set_friction(orc_t* o, double c) { o->friction = c; }
+
+int orc_set_equation(orc_t* o, int module, double p0, double p1)
+{
+    if (module < 0 || module >= PCL_EQ_COUNT) return ORC_ERR_BADARG;
+    o->eq = module;
+    o->eqp[0] = p0;
+    o->eqp[1] = p1;
+    return ORC_OK;
+}
 
 void orc_set_mesh(orc_t* o, const double* kappa, const double* lr_xi, const double* lr_eta)
 {

@@ -67,6 +67,9 @@ void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double
    friction), integrated by integrate_source_term (solver/MOD_solve.f90:295-336); c = 0 is the
    dam break's phi = 0 */
 void orc_set_friction(orc_t* o, double c);
+/* equation module of paraclaws_b200/csrc/pcl_equations.h (0: this oracle's own shallow-water
+   restatement); shallow water takes p0 = g, acoustics p0 = K, p1 = rho */
+int orc_set_equation(orc_t* o, int module, double p0, double p1);
 /* replace capacity and face length ratios by those of a mapped grid (finalize_mesh of a user
    mapping, SMOD_mesh_manipulation.f90:147-173); cell centres stay computational */
 void orc_set_mesh(orc_t* o, const double* kappa, const double* lr_xi, const double* lr_eta);

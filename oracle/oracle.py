@@ -68,6 +68,7 @@ def lib():
         L.orc_get_mesh.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
         L.orc_set_mesh.argtypes = [C.c_void_p, dp, dp, dp]
         L.orc_set_friction.argtypes = [C.c_void_p, C.c_double]
+        L.orc_set_equation.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
         L.orc_update_rank_boundaries.argtypes = [C.c_void_p]
         L.orc_solve_dimensional_split.argtypes = [C.c_void_p, P(C.c_int)]
         L.orc_sweep.argtypes = [C.c_void_p, C.c_int, P(C.c_double)]
@@ -182,6 +183,10 @@ class Oracle:
     def set_friction(self, c: float) -> None:
         """source_function phi = (0, -c hu, -c hv) (0: the dam break's phi = 0)."""
         lib().orc_set_friction(self.h, float(c))
+
+    def set_equation(self, module: int, p0: float = 0.0, p1: float = 0.0) -> None:
+        if lib().orc_set_equation(self.h, int(module), float(p0), float(p1)) != 0:
+            raise ValueError(f"unknown equation module {module}")
 
     def set_mesh(self, kappa, lr_xi, lr_eta) -> None:
         """Metrics of a mapped grid (arrays shaped like mesh()['kappa'])."""

@@ -107,6 +107,7 @@ def load(build_if_missing: bool = True):
     L.pcl_format_e26_16.argtypes = [C.c_double, C.c_char_p]
     L.pcl_set_user_bc.argtypes = [vp, vp, vp]
     L.pcl_set_source_hook.argtypes = [vp, vp, vp]
+    L.pcl_set_equation.argtypes = [vp, C.c_int, vp, C.c_int]
     L.pcl_compute_mesh_metrics.argtypes = [P(SolverControl), vp, vp, vp, vp, vp]
     L.pcl_update_time.argtypes = [vp, C.c_int]
     L.pcl_set_dt.argtypes = [vp, C.c_double]

@@ -87,6 +87,11 @@ _CONTROL_KINDS = {
 IC_FILE = 0          # raw float64 state in the reference layout, file initial_state.bin
 IC_CIRCULAR_DAM = 1  # examples/2D_dam_break/cartesian/SMOD_set_initial_conditions.f90:34-46
 
+# equation modules (include/paraclaws_b200.h PCL_EQ_*)
+EQ_SHALLOW_WATER = 0
+EQ_SHALLOW_WATER_GENERIC = 1
+EQ_ACOUSTICS = 2
+
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/paraclaws_b200.h"
+#include "pcl_equations.h"
 #include "pcl_launch.h"
 #include "pcl_types.h"
 #include "pcl_mixed.h"
@@ -833,8 +834,29 @@ static void drop_graph(pcl_ctx* x) {
   }
 }
 
+int pcl_set_equation(pcl_ctx* x, int module, const double* params, int nparams) {
+  if (!x || module < 0 || module >= PCL_EQ_COUNT || nparams < 0 || (nparams > 0 && !params)) return PCL_ERR_BADARG;
+  if (module != PCL_EQ_SHALLOW_WATER && (x->cfg.precision_mode != PCL_PREC_FP64 || x->g.metric == kMetricMapped))
+    return PCL_ERR_BADARG;
+  double p[2] = {x->cfg.grav, 0.0};
+  if (module == PCL_EQ_ACOUSTICS) {
+    if (nparams != 2 || !(params[0] > 0.0) || !(params[1] > 0.0)) return PCL_ERR_BADARG;
+    p[0] = params[0];
+    p[1] = params[1];
+  } else if (nparams >= 1) {
+    p[0] = params[0];
+  }
+  x->g.eq = module;
+  x->g.eqp[0] = p[0];
+  x->g.eqp[1] = p[1];
+  if (module == PCL_EQ_SHALLOW_WATER) x->g.grav = p[0];
+  drop_graph(x);
+  return PCL_OK;
+}
+
 int pcl_set_mesh_metrics(pcl_ctx* x, const double* capacity, const double* lrx, const double* lry) {
-  if (!x || !capacity || !lrx || !lry || x->cfg.precision_mode != PCL_PREC_FP64) return PCL_ERR_BADARG;
+  if (!x || !capacity || !lrx || !lry || x->cfg.precision_mode != PCL_PREC_FP64 || x->g.eq != PCL_EQ_SHALLOW_WATER)
+    return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   GridDev& g = x->g;
   const size_t ni = (size_t)g.mx + 4, nj = (size_t)g.my + 4;

@@ -24,17 +24,18 @@ constexpr int kYT = 128;   // columns of an eta-sweep CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 16;    // rows of an eta-sweep strip
 
+// MK values >= 16 select the generic equation-module path (GEN) with metric MK - 16.
 template <int NT, int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(NT, kXMinBlocks) xsweep_fp64_kernel(GridDev g) {
   __shared__ XSmem<NT> S;
   if (g.ctl->done) return;
-  xsweep_segment<NT, LIM, SO, MK>(g, 1 + blockIdx.y, 1 + blockIdx.x * (NT - 4), S);
+  xsweep_segment<NT, LIM, SO, MK % 16, (MK >= 16)>(g, 1 + blockIdx.y, 1 + blockIdx.x * (NT - 4), S);
 }
 
 template <int NTX, int STRIP, int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g) {
   if (g.ctl->done) return;
-  ysweep_strip<LIM, SO, MK>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
+  ysweep_strip<LIM, SO, MK % 16, (MK >= 16)>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
 }
 
 template <int LIM, bool SO, int MK>
@@ -60,6 +61,10 @@ void dispatch_lim(const GridDev& g, cudaStream_t st) {
 }
 template <template <int, bool, int> class F>
 void dispatch(const GridDev& g, cudaStream_t st) {
+  if (g.eq != PCL_EQ_SHALLOW_WATER) {  // generic modules: uniform grids (pcl_set_equation checks)
+    if (g.metric == kMetricUnit) return dispatch_lim<F, 16 + kMetricUnit>(g, st);
+    return dispatch_lim<F, 16 + kMetricTable>(g, st);
+  }
   if (g.metric == kMetricUnit) return dispatch_lim<F, kMetricUnit>(g, st);
   if (g.metric == kMetricMapped) return dispatch_lim<F, kMetricMapped>(g, st);
   return dispatch_lim<F, kMetricTable>(g, st);

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "pcl_equations.h"
 #include "pcl_types.h"
 
 namespace pcl {
@@ -82,6 +83,29 @@ __device__ __forceinline__ CellFlux cell_flux(double h, double hu, double hv, do
   if (isnan(jn) || isnan(d2) || isnan(jt) || isnan(d4) || isnan(d5)) *bad |= kStatusNaN;
   if (h < 0.0) *bad |= kStatusNegDepth;
   return c;
+}
+
+// Flux and wave-speed bound of a cell for any equation module (pcl_equations.h): J(q) from the
+// module, f = J.q in BLAS dgemv order (((0 + q1*J(:,1)) + q2*J(:,2)) + q3*J(:,3)), s = max |eig|.
+template <int DIR>
+__device__ __forceinline__ CellFlux cell_flux_generic(int module, double h, double hu, double hv, const double* prm,
+                                                      int* bad) {
+  const double q[3] = {h, hu, hv};
+  double J[9];
+  if (pcl_eq_jacobian(module, DIR + 1, q, prm, J)) *bad |= kStatusNaN;
+  double f[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double temp = q[c];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) f[r] = f[r] + temp * J[c * 3 + r];
+  }
+  double lam[3];
+  if (pcl_eq_eigenvalues(module, DIR + 1, q, prm, lam)) *bad |= kStatusNegDepth;
+  double s = fabs(lam[0]);
+  s = fabs(lam[1]) > s ? fabs(lam[1]) : s;
+  s = fabs(lam[2]) > s ? fabs(lam[2]) : s;
+  return CellFlux{f[0], f[1], f[2], s};
 }
 
 // HLL two-wave solve at one interface (SMOD_approximate_Riemann_solvers.f90:189-224):

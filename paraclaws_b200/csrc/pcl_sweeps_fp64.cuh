@@ -47,7 +47,8 @@ struct XSmem {
   double red[NT / 32];
 };
 
-template <int NT, int LIM, bool SO, int MK = kMetricTable>
+// GEN: a module other than the specialised shallow water (g.eq, pcl_equations.h)
+template <int NT, int LIM, bool SO, int MK = kMetricTable, bool GEN = false>
 __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   const Ctl* ctl = g.ctl;
@@ -78,7 +79,7 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
     if (c <= mx + 2) {
       const double h = q0[c + 1], hu = q1[c + 1], hv = q2[c + 1];
       int cb = 0;
-      const CellFlux F = cell_flux<0>(h, hu, hv, g.grav, &cb);
+      const CellFlux F = GEN ? cell_flux_generic<0>(g.eq, h, hu, hv, g.eqp, &cb) : cell_flux<0>(h, hu, hv, g.grav, &cb);
       if (c <= mx + 1) bad |= cb;  // getJakobi runs on cells -1 .. m_xi+1 in the xi sweep
       sq[0][t] = h; sq[1][t] = hu; sq[2][t] = hv;
       sf[0][t] = F.f0; sf[1][t] = F.f1; sf[2][t] = F.f2;
@@ -215,7 +216,7 @@ __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, con
   for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
 }
 
-template <int LIM, bool SO, int MK = kMetricTable>
+template <int LIM, bool SO, int MK = kMetricTable, bool GEN = false>
 __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   Ctl* ctl = g.ctl;
@@ -251,7 +252,8 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     c.q[1] = src[o + g.plane];
     c.q[2] = src[o + 2 * g.plane];
     int cb = 0;
-    c.F = cell_flux<1>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
+    c.F = GEN ? cell_flux_generic<1>(g.eq, c.q[0], c.q[1], c.q[2], g.eqp, &cb)
+              : cell_flux<1>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
     if (jj <= my + 1) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
     if constexpr (MP) {
       c.kap = __ldg(g.kap + o);

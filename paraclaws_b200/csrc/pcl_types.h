@@ -93,6 +93,8 @@ struct GridDev {
   int second_order, limiter; // limiter 0: unlimited correction; 1..4 by code
   int metric;                // kMetric*
   int user_bc;               // 1: sides coded 1 are filled by the host's user hook, not the wall
+  int eq;                    // equation module (pcl_equations.h); 0: the specialised shallow water
+  double eqp[2];             // its parameters (shallow water: g)
   double dxi, deta, area_scale /* d_xi*d_eta */, grav;
   // kMetricMapped only: per-cell metrics, cell (i, j) at [(j+1)*pitch + (i+1)]
   const double* kap;         // capacity(i, j)

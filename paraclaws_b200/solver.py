@@ -205,6 +205,12 @@ class Solver:
         None restores the built-in wall."""
         _lib.check(self.L.pcl_set_user_bc(self.h, fn_address, user), "pcl_set_user_bc")
 
+    def set_equation(self, module: int, params=()) -> None:
+        """Equation module (PCL_EQ_* of include/paraclaws_b200.h) and its parameters."""
+        arr = (C.c_double * max(len(params), 1))(*[float(p) for p in params])
+        _lib.check(self.L.pcl_set_equation(self.h, int(module), arr if params else None, len(params)),
+                   "pcl_set_equation")
+
     def set_source_hook(self, fn_address: Optional[int], user: Optional[int] = None) -> None:
         """Install a pcl_source_fn (integrate_source_term with a non-zero phi); None: phi = 0."""
         _lib.check(self.L.pcl_set_source_hook(self.h, fn_address, user), "pcl_set_source_hook")
