@@ -389,7 +389,8 @@ def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 30
     reference's flux J(q).q carries the pressure term g*h^2 (twice the shallow-water g*h^2/2),
     so its characteristic speeds are u +- sqrt(2 g h) while HLL and the CFL condition use
     u +- sqrt(g h); at CFL 0.9 the step amplifies rounding-level differences until they are
-    O(1e-2) after ~1000 steps, whatever arithmetic makes them."""
+    O(1e-2) after ~1000 steps, whatever arithmetic makes them.  The same curves at CFL 0.6, where
+    the step is well-conditioned, are reported beside."""
     import numpy as np
     import torch
 
@@ -397,55 +398,62 @@ def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 30
     from paraclaws_b200 import ic
     from paraclaws_b200.solver import Solver
     p = ic.seeded_dam_params(seed)
-    c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=1.0e9)
     cu = ctl.CustomSettings(max_accepted_steps=steps, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out)
     q = ic.circular_dam(m, m, p.radius, p.h_in, p.h_out, 0.0, 0.0)
     qp = q.copy()
     rng = np.random.Generator(np.random.PCG64(7))
     mask = rng.random(q.shape[:2]) < 0.01
     qp[..., 0] = np.where(mask, np.nextafter(q[..., 0], np.inf), q[..., 0])
-    runs = {"fp64": (ctl.PRECISION_FP64, q), "mixed": (ctl.PRECISION_MIXED, q), "fp64_perturbed": (ctl.PRECISION_FP64, qp)}
-    solvers = {}
-    sums0 = {}
-    for name, (prec, q0) in runs.items():
-        s = Solver(c, cu, device=device, precision=prec)
-        s.upload(q0)
-        s.update_rank_boundaries()
-        sums0[name] = s.conservation_sums()
-        solvers[name] = s
-    del qp
-    ms = {k: 0.0 for k in runs}
-    done = 0
-    curve = []
     names = ("h", "hu", "hv")
-    for cp in checkpoints:
+
+    def run(cfl, cps):
+        c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=1.0e9, cfl=cfl)
+        runs = {"fp64": (ctl.PRECISION_FP64, q), "mixed": (ctl.PRECISION_MIXED, q),
+                "fp64_perturbed": (ctl.PRECISION_FP64, qp)}
+        solvers, sums0 = {}, {}
+        for name, (prec, q0) in runs.items():
+            s = Solver(c, cu, device=device, precision=prec)
+            s.upload(q0)
+            s.update_rank_boundaries()
+            sums0[name] = s.conservation_sums()
+            solvers[name] = s
+        ms = {k: 0.0 for k in runs}
+        done = 0
+        curve = []
+        for cp in cps:
+            for name, s in solvers.items():
+                _, t_ms = _timed_advance(s, cp - done, torch)
+                ms[name] += t_ms
+            done = cp
+            ref = solvers["fp64"].download()[2:-2, 2:-2]
+            scale = float(np.abs(ref[..., 0]).sum())
+            row = {"step": cp, "time": solvers["fp64"].stats().time}
+            for name in ("mixed", "fp64_perturbed"):
+                x = solvers[name].download()[2:-2, 2:-2]
+                row[name] = {"l1_rel": {names[k]: float(np.abs(x[..., k] - ref[..., k]).sum() / scale) for k in range(3)},
+                             "linf": {names[k]: float(np.abs(x[..., k] - ref[..., k]).max()) for k in range(3)}}
+                del x
+            curve.append(row)
+            del ref
+        out = {}
         for name, s in solvers.items():
-            st, t_ms = _timed_advance(s, cp - done, torch)
-            ms[name] += t_ms
-        done = cp
-        ref = solvers["fp64"].download()[2:-2, 2:-2]
-        scale = float(np.abs(ref[..., 0]).sum())
-        row = {"step": cp, "time": solvers["fp64"].stats().time}
-        for name in ("mixed", "fp64_perturbed"):
-            x = solvers[name].download()[2:-2, 2:-2]
-            row[name] = {"l1_rel": {names[k]: float(np.abs(x[..., k] - ref[..., k]).sum() / scale) for k in range(3)},
-                         "linf": {names[k]: float(np.abs(x[..., k] - ref[..., k]).max()) for k in range(3)}}
-            del x
-        curve.append(row)
-        del ref
-    out = {}
-    for name, s in solvers.items():
-        st = s.stats()
-        m1 = s.conservation_sums()
-        out[name] = {"value": st.accepted * m * m / (ms[name] * 1e-3), "ms": ms[name], "time": st.time,
-                     "accepted": st.accepted, "rejected": st.rejected,
-                     "mass_drift_rel": float((m1[0] - sums0[name][0]) / sums0[name][0])}
-        s.close()
+            st = s.stats()
+            m1 = s.conservation_sums()
+            out[name] = {"value": st.accepted * m * m / (ms[name] * 1e-3), "ms": ms[name], "time": st.time,
+                         "accepted": st.accepted, "rejected": st.rejected,
+                         "mass_drift_rel": float((m1[0] - sums0[name][0]) / sums0[name][0])}
+            s.close()
+        return out, curve
+
+    out, curve = run(0.9, checkpoints)
     last = curve[-1]
     out["l1_rel"] = last["mixed"]["l1_rel"]
     out["linf"] = last["mixed"]["linf"]
     out["conditioning_floor_l1_rel"] = last["fp64_perturbed"]["l1_rel"]
     out["curve"] = curve
+    _, curve06 = run(0.6, (200, 500, 1000))
+    out["curve_cfl_0_6"] = [{"step": r["step"], "mixed_l1_h": r["mixed"]["l1_rel"]["h"],
+                             "fp64_perturbed_l1_h": r["fp64_perturbed"]["l1_rel"]["h"]} for r in curve06]
     out["workload"] = (f"{m}^2 seeded dam break (seed {seed}: radius {p.radius:.3f}, h_in/h_out {p.h_in:.3f}), "
                        f"minmod, CFL 0.9, {steps} accepted steps")
     out["note"] = ("L1 of each component relative to sum|h| of the FP64 result, Linf absolute; "

@@ -231,6 +231,7 @@ int pcl_read_solver_control(const char* control_in, const char* custom_in, pcl_s
 int validate_control(const pcl_solver_control* c) {
   if (c->num_equations != 3 || c->num_waves != 2 || c->num_ghost != 2) return PCL_ERR_BADARG;
   if (c->m_xi < 2 || c->m_eta < 2) return PCL_ERR_BADARG;
+  if (c->m_xi > (1 << 28) || c->m_eta > 16 * 65535) return PCL_ERR_BADARG;  // launch-grid limits
   const int bcs[4] = {c->bc_xi_lower, c->bc_xi_upper, c->bc_eta_lower, c->bc_eta_upper};
   for (int k = 0; k < 4; ++k)
     if (bcs[k] < 1 || bcs[k] > 3) return PCL_ERR_BADARG;

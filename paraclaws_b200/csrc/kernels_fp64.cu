@@ -29,7 +29,11 @@ template <int NT, int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(NT, kXMinBlocks) xsweep_fp64_kernel(GridDev g) {
   __shared__ XSmem<NT> S;
   if (g.ctl->done) return;
-  xsweep_segment<NT, LIM, SO, MK % 16, (MK >= 16)>(g, 1 + blockIdx.y, 1 + blockIdx.x * (NT - 4), S);
+  // one row per blockIdx.y, strided when the grid has more rows than gridDim.y allows
+  for (int j = 1 + blockIdx.y; j <= g.my; j += gridDim.y) {
+    xsweep_segment<NT, LIM, SO, MK % 16, (MK >= 16)>(g, j, 1 + blockIdx.x * (NT - 4), S);
+    if (j + gridDim.y <= g.my) __syncthreads();  // the shared arrays are reused by the next row
+  }
 }
 
 template <int NTX, int STRIP, int LIM, bool SO, int MK>
@@ -40,7 +44,7 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
 
 template <int LIM, bool SO, int MK>
 void launch_x_t(const GridDev& g, cudaStream_t st) {
-  dim3 gx((g.mx + (kXT - 4) - 1) / (kXT - 4), g.my);
+  dim3 gx((g.mx + (kXT - 4) - 1) / (kXT - 4), g.my < 65535 ? g.my : 65535);
   xsweep_fp64_kernel<kXT, LIM, SO, MK><<<gx, kXT, 0, st>>>(g);
 }
 template <int LIM, bool SO, int MK>

@@ -162,3 +162,18 @@ def test_bad_state_is_reported(pcl, kind):
     with pytest.raises(PclError) as e:
         s.advance()
     assert e.value.code == (PCL_ERR_NAN if kind == "nan" else PCL_ERR_NEG_DEPTH)
+
+
+def test_tall_grid_beyond_one_launch_row_per_block(pcl, oracle_lib):
+    """More rows than one xi-sweep launch has blocks in y (65535): the kernel strides over rows."""
+    c = dataclasses.replace(ctl.dam_break_control(6, limiter=1, bc=2, time_final=1.0), m_eta=70000,
+                            eta_min=-1.0, eta_max=1.0 + 69994 * (2.0 / 6))
+    q = ic.gaussian_bumps(6, 70000, seed=5)
+    s, o = _pair(c)
+    _start(s, o, q)
+    s.advance(max_attempts=3)
+    log_o = o.run(max_attempts=3)
+    assert np.array_equal(s.step_log().dt, log_o.dt)
+    _assert_state_equal(s.download(), o.state(), "tall grid")
+    s.close()
+    o.close()
