@@ -3,11 +3,12 @@
  *
  * The drop-in boundary for paraCLAWs' hot path: the Fortran host keeps read_solver_control,
  * the user equation module and the time loop of main.f90, and binds these entry points with
- * iso_c_binding (bind(C) interfaces: see INTEGRATION.md).  Plain C types only; all arrays
+ * iso_c_binding (one bind(C) interface per function below).  Plain C types only; all arrays
  * are caller-owned host buffers; every call returns an int status (PCL_OK = 0, errors < 0).
  *
  * Threading: one host thread per context; each context owns one CUDA stream and its device
- * memory; there is no global state besides the CUDA device.
+ * memory.  The only state shared between contexts is the static device scratch of
+ * pcl_solve_dimensional_split_noalloc.
  *
  * State layout at the boundary is the reference's: vars(3, -1:m_xi+2, -1:m_eta+2) column-major
  * (domain/SMOD_domain_allocation.f90:94), (h, hu, hv) fastest.  Inside the context the state is
