@@ -32,7 +32,7 @@ extern "C" {
 #define PCL_ERR_FATAL_DT (-7)   /* end_program in updateTime (time_control/MOD_time_control.f90:213-231) */
 #define PCL_ERR_IO (-8)         /* control.in / custom.in unreadable, or a snapshot file unwritable */
 #define PCL_ERR_FULL (-9)       /* batch: no free slot or over the memory budget */
-#define PCL_ERR_USER (-10)      /* the user boundary hook returned an error */
+#define PCL_ERR_USER (-10)      /* a device hook (user boundary condition, source term) failed */
 
 /* precision forms (custom.in) */
 #define PCL_PREC_FP64 0   /* bit-compatible FP64 path (the drop-in) */

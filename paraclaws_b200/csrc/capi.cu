@@ -90,7 +90,7 @@ const char* pcl_status_string(int s) {
     case PCL_ERR_FATAL_DT: return "time step control cannot continue (constant dt violated)";
     case PCL_ERR_IO: return "cannot read a control file or write a snapshot file";
     case PCL_ERR_FULL: return "batch is full or over its memory budget";
-    case PCL_ERR_USER: return "the user boundary hook failed";
+    case PCL_ERR_USER: return "a device hook (user boundary condition or source term) failed";
     default: return "unknown status";
   }
 }

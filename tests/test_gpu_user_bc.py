@@ -159,7 +159,7 @@ def test_failing_hook_is_reported(pcl, userlib):
     s.initial_condition()
     with pytest.raises(_lib.PclError) as e:
         s.update_rank_boundaries()
-    assert "user boundary hook" in str(e.value)
+    assert "device hook" in str(e.value)
     s.set_user_bc(None)
     s.update_rank_boundaries()
     s.close()
