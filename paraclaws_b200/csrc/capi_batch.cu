@@ -78,6 +78,8 @@ struct pcl_batch {
   int n_items = 0;
   // schedule (the autotuner's knobs)
   int x_rows = 4, y_rows = 16, tile_rows = 64, blocks_per_sm = 0;
+  int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
+  int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   long long launches = 0;
@@ -118,6 +120,7 @@ static BatchView view(const pcl_batch* b) {
   v.x_rows = b->x_rows;
   v.y_rows = b->y_rows;
   v.tile_rows = b->tile_rows;
+  v.desc_base = b->desc_base;
   v.spin_limit = 1u << 24;
   return v;
 }
@@ -125,7 +128,8 @@ static BatchView view(const pcl_batch* b) {
 static int grid_size(const pcl_batch* b) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  const int occ = b->precision == PCL_PREC_MIXED ? batch_mixed_occupancy() : batch_fp64_occupancy();
+  const int occ =
+      b->precision == PCL_PREC_MIXED ? batch_mixed_occupancy(b->desc_base >= 0, b->mode) : batch_fp64_occupancy();
   const int per = b->blocks_per_sm > 0 ? std::min(b->blocks_per_sm, occ) : occ;
   return sms * per;
 }
@@ -143,6 +147,15 @@ static int rebuild_items(pcl_batch* b) {
   std::vector<int4> items;
   std::vector<int> totals(2 * b->slots.size(), 0);
   if (b->precision == PCL_PREC_MIXED) {
+    int mode = -2;
+    for (int s : order) {
+      const GridDev& g = b->slots[s].g;
+      const int m = g.second_order ? 1 + g.limiter : 0;
+      mode = mode == -2 ? m : (mode == m ? m : -1);
+    }
+    if (mode < 0) mode = -1;
+    if (mode != b->mode) drop_graph(b);  // the captured launches run the other build
+    b->mode = mode;
     for (int s : order) {
       const auto& c = b->slots[s].cfg;
       const int ns = (c.m_xi + kMixedStrip - 1) / kMixedStrip, nr = (c.m_eta + b->tile_rows - 1) / b->tile_rows;
@@ -190,7 +203,7 @@ static void enqueue_step(pcl_batch* b) {
   cudaMemsetAsync(b->scal_d + 1, 0, sizeof(int), b->stream);
   const BatchView v = view(b);
   if (b->precision == PCL_PREC_MIXED)
-    launch_batch_mixed(v, grid_size(b), b->stream);
+    launch_batch_mixed(v, grid_size(b), b->desc_base >= 0, b->mode, b->stream);
   else
     launch_batch_fp64(v, grid_size(b), b->stream);
 }
@@ -232,6 +245,9 @@ int pcl_batch_create(int device, int precision, int max_instances, pcl_batch** o
   cudaMemsetAsync(b->counters_d, 0, sizeof(int) * 2 * max_instances, b->stream);
   cudaMemsetAsync(b->totals_d, 0, sizeof(int) * 2 * max_instances, b->stream);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) return fail(PCL_ERR_CUDA);
+  // a mixed batch takes a range of the constant descriptor pool if one is free (else its items
+  // read their descriptors from global memory)
+  if (precision == PCL_PREC_MIXED) b->desc_base = batch_desc_reserve(max_instances);
   *out = b;
   return PCL_OK;
 }
@@ -252,6 +268,7 @@ int pcl_batch_destroy(pcl_batch* b) {
   cudaFree(b->staging_d);
   cudaFreeHost(b->ctl_h);
   cudaStreamDestroy(b->stream);
+  if (b->desc_base >= 0) batch_desc_release(b->desc_base, (int)b->slots.size());
   delete b;
   return PCL_OK;
 }
@@ -332,6 +349,19 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   BCK(cudaStreamSynchronize(b->stream));
   g.metric = h->nonunit_metric ? kMetricTable : kMetricUnit;
   BCK(cudaMemcpyAsync(b->inst_d + s, &g, sizeof(GridDev), cudaMemcpyHostToDevice, b->stream));
+  if (b->desc_base >= 0) {
+    ItemDesc d{};
+    d.state = g.state;
+    d.bufstride = g.bufstride;
+    d.plane = g.plane;
+    d.ctl = g.ctl;
+    d.grav = g.grav;
+    d.mx = g.mx;
+    d.my = g.my;
+    d.pitch = g.pitch;
+    d.mode = g.second_order ? 1 + g.limiter : 0;
+    BCK(batch_mixed_set_desc(b->desc_base + s, d, b->stream));
+  }
   BCK(cudaGetLastError());
   BCK(cudaStreamSynchronize(b->stream));
   sl.used = true;

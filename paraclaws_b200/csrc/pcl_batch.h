@@ -18,6 +18,19 @@ namespace pcl {
 
 enum : int { kItemX = 0, kItemY = 1, kItemMixed = 2 };
 
+// The fields of GridDev one mixed item reads.  A batch that owns a range of the constant-memory
+// pool keeps its instances' descriptors there: loads from the constant bank can be repeated
+// instead of held in registers, so the persistent kernel fits five CTAs per SM.
+struct ItemDesc {
+  double* state;
+  long long bufstride, plane;
+  Ctl* ctl;
+  double grav;
+  int mx, my, pitch;
+  int mode;  // 0: first order; else 1 + limiter (0: unlimited correction, 1..4 by code)
+};
+constexpr int kDescPool = 1024;  // descriptors in the pool (56 KB of constant memory)
+
 struct BatchView {
   const GridDev* inst;   // [max_slots]
   const int4* items;     // [n_items]
@@ -28,16 +41,26 @@ struct BatchView {
   int x_rows;            // rows per FP64 xi item
   int y_rows;            // rows per FP64 eta strip
   int tile_rows;         // rows per mixed item
+  int desc_base;         // first pool descriptor of this batch (mixed, pool build only)
   unsigned spin_limit;   // bounded waits of eta items for their xi items
 };
 
 void launch_batch_fp64(const BatchView& v, int grid, cudaStream_t st);
-void launch_batch_mixed(const BatchView& v, int grid, cudaStream_t st);
+// pool = true: item descriptors from the constant pool at v.desc_base (the builds for five CTAs
+// per SM); false: from v.inst in global memory.  mode 0..5 (ItemDesc::mode): every instance has
+// that mode and the pool build specialised for it runs; -1: any mix.
+void launch_batch_mixed(const BatchView& v, int grid, bool pool, int mode, cudaStream_t st);
+// copy one descriptor into the pool (stream-ordered with the launches)
+cudaError_t batch_mixed_set_desc(int index, const ItemDesc& d, cudaStream_t st);
+// reserve n consecutive pool descriptors on the current device: the first index, or -1 if
+// there is no room; release them again
+int batch_desc_reserve(int n);
+void batch_desc_release(int base, int n);
 int batch_fp64_threads();   // also the columns of an FP64 eta item
 int batch_fp64_segment();   // cells of an FP64 xi item's row segment
 int batch_mixed_threads();
 // largest number of resident CTAs per SM of each persistent kernel
 int batch_fp64_occupancy();
-int batch_mixed_occupancy();
+int batch_mixed_occupancy(bool pool, int mode);
 
 }  // namespace pcl

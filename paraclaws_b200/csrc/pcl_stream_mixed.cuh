@@ -159,8 +159,10 @@ __device__ __forceinline__ WF load_wf(const Smem& S, int s) {
 // UNROLL unrolls the row loop (the single-grid kernel: 2, letting the eta window shift by
 // renaming; the batched kernel: 1, which keeps its register count at four CTAs per SM).  It
 // changes no arithmetic.
-template <int LIM, bool SO, int UNROLL = 1>
-__device__ __forceinline__ bool mixed_item(const GridDev& g, int strip, int seg, int TY, Smem& S, unsigned& rows) {
+// G is GridDev or any descriptor with its fields ctl, grav, mx, my, pitch, plane, state and
+// bufstride (the batch keeps a compact one in constant memory).
+template <int LIM, bool SO, int UNROLL = 1, class G>
+__device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int TY, Smem& S, unsigned& rows) {
   Ctl* ctl = g.ctl;
   const int t = threadIdx.x;
   const int cur = ctl->cur;
@@ -175,11 +177,11 @@ __device__ __forceinline__ bool mixed_item(const GridDev& g, int strip, int seg,
   const int j1 = min(j0 + TY - 1, my);
   const int c0 = i0 - 1;  // storage column of cell i0-2 (even: 16-byte aligned)
   const int ncopy = min(NT, (int)(P - c0));
-  const double* in = buffer(g, cur);
+  const double* in = g.state + (long long)cur * g.bufstride;
   const int jfirst = j0 - 2, nrows = (j1 + 2) - jfirst + 1;
   const int icol = i0 + t;                    // this thread's column in the eta sweep
   const bool ycol = t < TXI && icol <= mx;
-  double* outp = buffer(g, ob) + (icol + 1);
+  double* outp = g.state + (long long)ob * g.bufstride + (icol + 1);
 
   const unsigned base = rows;
   auto issue = [&](int row, int slot) {

@@ -77,6 +77,24 @@ def test_schedule_does_not_change_results(pcl, precision):
         assert np.array_equal(a, c)
 
 
+def test_descriptor_pool_and_global_descriptors_agree(pcl):
+    """A mixed batch reads its item descriptors from the constant-memory pool (1024 entries);
+    one with more slots than the pool holds reads them from global memory through another build
+    of the kernel.  Both give the same bits, also while the first batch holds its pool range."""
+    inst = _instances(6, seed=11)
+    results = []
+    pooled = Batch(8, precision=ctl.PRECISION_MIXED)
+    unpooled = Batch(1100, precision=ctl.PRECISION_MIXED)
+    for b in (pooled, unpooled):
+        slots = [b.add(c, q) for c, q in inst]
+        b.step(60)
+        results.append([b.download(s) for s in slots])
+    pooled.close()
+    unpooled.close()
+    for a, c in zip(results[0], results[1]):
+        assert np.array_equal(a, c)
+
+
 def test_add_and_remove_between_steps(pcl):
     """Membership changes between steps: a new instance starts from its own initial state and
     ends bit-identical to running alone, even though it joined mid-flight."""
@@ -95,6 +113,41 @@ def test_add_and_remove_between_steps(pcl):
             break
     for s, k in ((s0, 0), (s2, 2), (s3, 3)):
         qa, _ = _alone(*inst[k], ctl.PRECISION_MIXED)
+        assert np.array_equal(b.download(s), qa)
+    b.close()
+
+
+@pytest.mark.parametrize("first_mode", ["first_order", "unlimited", 1, 2, 3, 4])
+def test_single_mode_builds_and_switch_to_mixed_modes(pcl, first_mode):
+    """While every instance of a mixed batch has the same flux mode (first order, unlimited
+    correction, or one limiter) the kernel built for that mode alone runs; adding an instance of
+    another mode switches the batch to the build for any mix.  Every instance still ends
+    bit-identical to running alone."""
+    base = _instances(4, seed=5)
+    same = []
+    for c, q in base[:3]:
+        if first_mode == "first_order":
+            c = dataclasses.replace(c, add_higher_order_flux_correction=False)
+        elif first_mode == "unlimited":
+            c = dataclasses.replace(c, use_limtiter=False)
+        else:
+            c = dataclasses.replace(c, limiter_function=first_mode)
+        same.append((c, q))
+    c3, q3 = base[3]
+    other = (dataclasses.replace(c3, limiter_function=1 if first_mode == 4 else 4), q3)
+    b = Batch(4, precision=ctl.PRECISION_MIXED)
+    slots = [b.add(c, q) for c, q in same]
+    b.step(40)  # one captured chunk of the single-mode build plus single launches
+    slots.append(b.add(*other))
+    cases = same + [other]
+    for _ in range(200):
+        b.step(16)
+        done, _ = b.poll()
+        if all(done[s] == 1 for s in slots):
+            break
+    for s, (c, q) in zip(slots, cases):
+        qa, la = _alone(c, q, ctl.PRECISION_MIXED)
+        assert np.array_equal(b.step_log(s).dt, la.dt)
         assert np.array_equal(b.download(s), qa)
     b.close()
 
