@@ -77,7 +77,8 @@ struct pcl_batch {
   bool dirty = true;
   int n_items = 0;
   // schedule (the autotuner's knobs)
-  int x_rows = 4, y_rows = 16, tile_rows = 64, blocks_per_sm = 0;
+  int x_rows = 4, y_rows = 16, tile_rows = 0, blocks_per_sm = 0;  // tile_rows 0: chosen per membership
+  int tile_rows_eff = 64;  // rows per mixed item in the current items (a launch parameter)
   int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
   int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
   cudaGraphExec_t graph = nullptr;
@@ -119,7 +120,7 @@ static BatchView view(const pcl_batch* b) {
   v.totals = b->totals_d;
   v.x_rows = b->x_rows;
   v.y_rows = b->y_rows;
-  v.tile_rows = b->tile_rows;
+  v.tile_rows = b->tile_rows_eff;
   v.desc_base = b->desc_base;
   v.spin_limit = 1u << 24;
   return v;
@@ -132,6 +133,32 @@ static int grid_size(const pcl_batch* b) {
       b->precision == PCL_PREC_MIXED ? batch_mixed_occupancy(b->desc_base >= 0, b->mode) : batch_fp64_occupancy();
   const int per = b->blocks_per_sm > 0 ? std::min(b->blocks_per_sm, occ) : occ;
   return sms * per;
+}
+
+// Rows per mixed item when the schedule leaves it open (tile_rows 0): the height that minimises
+// the estimated step time, waves x (rows an item streams + a fixed cost per item), where waves
+// is the item count over the persistent CTAs, rounded up.  A few small instances get short
+// items spread over the SMs (a step takes about one item's time); a large batch gets taller
+// items whose four halo rows cost less.
+constexpr int kItemFixedRows = 8;
+
+static int auto_tile_rows(const pcl_batch* b, const std::vector<int>& order) {
+  const long long ctas = std::max(1, grid_size(b));
+  int best = 64;
+  double best_cost = 1e300;
+  for (int ty : {16, 32, 64, 128, 256}) {
+    long long n = 0;
+    for (int s : order) {
+      const auto& c = b->slots[s].cfg;
+      n += (long long)((c.m_xi + kMixedStrip - 1) / kMixedStrip) * ((c.m_eta + ty - 1) / ty);
+    }
+    const double cost = (double)((n + ctas - 1) / ctas) * (ty + 4 + kItemFixedRows);
+    if (cost <= best_cost) {  // ties: the taller item (fewer of them)
+      best_cost = cost;
+      best = ty;
+    }
+  }
+  return best;
 }
 
 // Work items of every used slot, largest instances first so the long items start early.
@@ -153,12 +180,21 @@ static int rebuild_items(pcl_batch* b) {
       const int m = g.second_order ? 1 + g.limiter : 0;
       mode = mode == -2 ? m : (mode == m ? m : -1);
     }
-    if (mode < 0) mode = -1;
-    if (mode != b->mode) drop_graph(b);  // the captured launches run the other build
-    b->mode = mode;
+    // an empty batch keeps its build (and its captured graph) for the next instance
+    if (mode != -2) {
+      if (mode < 0) mode = -1;
+      if (mode != b->mode) drop_graph(b);  // the captured launches run the other build
+      b->mode = mode;
+    }
+    if (!order.empty()) {
+      const int ty = b->tile_rows > 0 ? b->tile_rows : auto_tile_rows(b, order);
+      if (ty != b->tile_rows_eff) drop_graph(b);  // the captured launches carry the old height
+      b->tile_rows_eff = ty;
+    }
     for (int s : order) {
       const auto& c = b->slots[s].cfg;
-      const int ns = (c.m_xi + kMixedStrip - 1) / kMixedStrip, nr = (c.m_eta + b->tile_rows - 1) / b->tile_rows;
+      const int ns = (c.m_xi + kMixedStrip - 1) / kMixedStrip;
+      const int nr = (c.m_eta + b->tile_rows_eff - 1) / b->tile_rows_eff;
       for (int r = 0; r < nr; ++r)
         for (int k = 0; k < ns; ++k) items.push_back(make_int4(s, kItemMixed, k, r));
       totals[2 * s + 1] = ns * nr;
@@ -385,7 +421,7 @@ int pcl_batch_remove(pcl_batch* b, int s) {
 }
 
 int pcl_batch_set_schedule(pcl_batch* b, int tile_rows, int x_rows, int y_rows, int blocks_per_sm) {
-  if (!b || tile_rows < 4 || x_rows < 1 || y_rows < 1 || blocks_per_sm < 0) return PCL_ERR_BADARG;
+  if (!b || (tile_rows != 0 && tile_rows < 4) || x_rows < 1 || y_rows < 1 || blocks_per_sm < 0) return PCL_ERR_BADARG;
   b->tile_rows = tile_rows;
   b->x_rows = x_rows;
   b->y_rows = y_rows;

@@ -13,20 +13,29 @@ namespace pcl {
 
 __device__ __forceinline__ int ghost_items(const GridDev& g) { return 8 * max(g.mx, g.my); }
 
-__device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid) {
+// One ghost cell's three values and where they go (plane 0; plane p at dst + p * plane).
+struct GhostVal {
+  double* dst;
+  double v[3];
+};
+
+// Loads only: no ghost item reads a cell that another one writes (sources are interior cells
+// and the metric tables), so the three planes of an item are all loaded before any is stored
+// (one memory round trip per item, not one per plane).  Returns false where it writes nothing.
+__device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid, GhostVal& o) {
   const int mx = g.mx, my = g.my;
   const int n = max(mx, my);
   const int side = tid / (2 * n);
   const int rem = tid - side * 2 * n;
   const int layer = rem / n;
   const int idx = 1 + rem - layer * n;  // 1-based position along the side
-  if (side >= 4) return;
+  if (side >= 4) return false;
   const long long P = g.pitch;
   const int bc = g.bc[side];
-  if (bc == 1 && g.user_bc) return;  // the user boundary hook fills this side
+  if (bc == 1 && g.user_bc) return false;  // the user boundary hook fills this side
   if (side < 2) {  // xi boundaries, rows j = 1 .. m_eta
     const int j = idx;
-    if (j > my) return;
+    if (j > my) return false;
     const int i = side == 0 ? -1 + layer : mx + 1 + layer;
     const int i1 = side == 0 ? 1 : mx;          // nearest interior cell
     const int i2 = side == 0 ? 2 : mx - 1;      // second interior cell
@@ -34,8 +43,10 @@ __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid)
     const double xg = __ldg(g.colm + (i + 1) * kColMetrics + 3);
     const double x1 = __ldg(g.colm + (i1 + 1) * kColMetrics + 3);
     const double x2 = __ldg(g.colm + (i2 + 1) * kColMetrics + 3);
+    o.dst = b + (long long)(j + 1) * P + (i + 1);
+#pragma unroll
     for (int me = 0; me < 3; ++me) {
-      double* p = b + me * g.plane + (long long)(j + 1) * P;
+      const double* p = b + me * g.plane + (long long)(j + 1) * P;
       double v;
       if (bc == 2) {
         v = p[i1 + 1];
@@ -50,11 +61,11 @@ __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid)
       } else {
         v = me == 1 ? -p[im + 1] : p[im + 1];
       }
-      p[i + 1] = v;
+      o.v[me] = v;
     }
   } else {  // eta boundaries, columns i = 1 .. m_xi
     const int i = idx;
-    if (i > mx) return;
+    if (i > mx) return false;
     const int j = side == 2 ? -1 + layer : my + 1 + layer;
     const int j1 = side == 2 ? 1 : my;
     const int j2 = side == 2 ? 2 : my - 1;
@@ -62,8 +73,10 @@ __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid)
     const double yg = __ldg(g.rowm + (j + 1) * kRowMetrics + 3);
     const double y1 = __ldg(g.rowm + (j1 + 1) * kRowMetrics + 3);
     const double y2 = __ldg(g.rowm + (j2 + 1) * kRowMetrics + 3);
+    o.dst = b + (long long)(j + 1) * P + (i + 1);
+#pragma unroll
     for (int me = 0; me < 3; ++me) {
-      double* p = b + me * g.plane + (i + 1);
+      const double* p = b + me * g.plane + (i + 1);
       double v;
       if (bc == 2) {
         v = p[(long long)(j1 + 1) * P];
@@ -76,9 +89,21 @@ __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid)
       } else {
         v = me == 2 ? -p[(long long)(jm + 1) * P] : p[(long long)(jm + 1) * P];
       }
-      p[(long long)(j + 1) * P] = v;
+      o.v[me] = v;
     }
   }
+  return true;
+}
+
+__device__ __forceinline__ void ghost_store(const GridDev& g, const GhostVal& o) {
+  o.dst[0] = o.v[0];
+  o.dst[g.plane] = o.v[1];
+  o.dst[2 * g.plane] = o.v[2];
+}
+
+__device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid) {
+  GhostVal o;
+  if (ghost_value(g, b, tid, o)) ghost_store(g, o);
 }
 
 }  // namespace pcl

@@ -64,7 +64,8 @@ def test_batch_equals_alone(pcl, precision):
 def test_schedule_does_not_change_results(pcl, precision):
     inst = _instances(5, seed=7)
     results = []
-    scheds = ([Schedule(tile_rows=16), Schedule(tile_rows=128, blocks_per_sm=1)] if precision == ctl.PRECISION_MIXED
+    scheds = ([Schedule(tile_rows=16), Schedule(tile_rows=128, blocks_per_sm=1), Schedule(tile_rows=0)]
+              if precision == ctl.PRECISION_MIXED
               else [Schedule(x_rows=4, y_rows=16), Schedule(x_rows=16, y_rows=64, blocks_per_sm=1)])
     for sch in scheds:
         b = Batch(8, precision=precision)
@@ -73,8 +74,9 @@ def test_schedule_does_not_change_results(pcl, precision):
         b.step(40)
         results.append([b.download(s) for s in slots])
         b.close()
-    for a, c in zip(results[0], results[1]):
-        assert np.array_equal(a, c)
+    for other in results[1:]:
+        for a, c in zip(results[0], other):
+            assert np.array_equal(a, c)
 
 
 def test_descriptor_pool_and_global_descriptors_agree(pcl):
