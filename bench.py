@@ -462,7 +462,7 @@ def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 30
     return out
 
 
-def form_batch(device, n=512, steps=32):
+def form_batch(device, n=512, steps=32, precisions=("fp64", "mixed")):
     """512 dam-break instances, sides log-uniform 64..1024 (multiples of 32), own dt each."""
     import torch
 
@@ -472,6 +472,8 @@ def form_batch(device, n=512, steps=32):
     sides = ic.log_uniform_sides(n, 64, 1024, 32, seed=2)
     res = {}
     for name, prec in (("fp64", ctl.PRECISION_FP64), ("mixed", ctl.PRECISION_MIXED)):
+        if name not in precisions:
+            continue
         b = Batch(n, precision=prec, device=device)
         for k, m in enumerate(sides):
             p = ic.seeded_dam_params(k, offset=0.25)
@@ -723,10 +725,18 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the mixed/batch/serving/precision forms")
+    ap.add_argument("--form", choices=["batch"], help="run only this form and print its result (profiling)")
+    ap.add_argument("--instances", type=int, default=512, help="--form batch: number of grids")
+    ap.add_argument("--batch-precision", choices=["fp64", "mixed", "both"], default="both")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.form == "batch":
+        import torch
+        torch.cuda.set_device(0)
+        prec = ("fp64", "mixed") if args.batch_precision == "both" else (args.batch_precision,)
+        print(json.dumps({"form": "batch", **form_batch(0, n=args.instances, precisions=prec)}), flush=True)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
