@@ -49,10 +49,62 @@ __device__ __forceinline__ void mode_item(const G& g, int strip, int seg, int ty
 
 __device__ __forceinline__ int item_mode(const GridDev& g) { return g.second_order ? 1 + g.limiter : 0; }
 
+// Ghost cells (update_rank_boundaries) filled by the items themselves, when the batch is small
+// enough that its step time is a few items' latency (the IG builds; with many items the
+// finishing CTA's fill overlaps other CTAs' items and costs less).  Same values either way.  A ghost value reads
+// interior cells within two cells of its side, of the buffer the step writes.  An item that
+// wrote those cells fills that side's ghosts along its own rows (xi sides) or columns (eta
+// sides) once its rows are done, before its completion count.  They go into the step's output
+// buffer whether or not the step is then accepted: a rejected step leaves that buffer unused.
+// Only the high side of a grid whose last strip (segment) is one column (row) wide has its two
+// source cells in different items; the finishing CTA fills that one (finisher_ghosts).
+__device__ __forceinline__ void item_ghosts(const GridDev& g, int strip, int seg, int ty) {
+  const int mx = g.mx, my = g.my, n = max(mx, my);
+  const int cur = g.ctl->cur;
+  double* b = buffer(g, cur == 0 ? 2 : cur - 1);
+  const int i0 = 1 + strip * mixed::TXI, i1 = min(i0 + mixed::TXI - 1, mx);
+  const int j0 = 1 + seg * ty, j1 = min(j0 + ty - 1, my);
+  const int nc = i1 - i0 + 1, nr = j1 - j0 + 1;
+  const int c0 = strip == 0 ? 2 * nr : 0;                // xi low: sources i = 1, 2
+  const int c1 = i1 == mx && nc >= 2 ? 2 * nr : 0;       // xi high: i = mx, mx - 1
+  const int c2 = seg == 0 ? 2 * nc : 0;                  // eta low: j = 1, 2
+  const int c3 = j1 == my && nr >= 2 ? 2 * nc : 0;       // eta high: j = my, my - 1
+  const int total = c0 + c1 + c2 + c3;
+  for (int k = threadIdx.x; k < total; k += blockDim.x) {
+    int side = 0, r = k;
+    if (r >= c0) { r -= c0; side = 1;
+      if (r >= c1) { r -= c1; side = 2;
+        if (r >= c2) { r -= c2; side = 3; } } }
+    const int len = side < 2 ? nr : nc;
+    const int layer = r / len;
+    const int pos = (side < 2 ? j0 : i0) + (r - layer * len);  // 1-based along the side
+    ghost_item(g, b, side * 2 * n + layer * n + (pos - 1));
+  }
+}
+
+// True for an item on the edge of its grid (first or last strip or segment): only those write
+// ghost cells, and the rest skip item_ghosts without reading the grid's descriptor.
+__device__ __forceinline__ bool edge_item(int mx, int my, int strip, int seg, int ty) {
+  return strip == 0 || seg == 0 || (strip + 1) * mixed::TXI >= mx || (seg + 1) * ty >= my;
+}
+
+// The sides item_ghosts leaves open, after an accepted step (b: the new current buffer).
+__device__ __forceinline__ void finisher_ghosts(const GridDev& g, int ty, double* b) {
+  const int n = max(g.mx, g.my);
+  const bool xi_hi = (g.mx - 1) % mixed::TXI == 0;  // last strip one column wide
+  const bool eta_hi = (g.my - 1) % ty == 0;         // last segment one row high
+  for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) {
+    if (xi_hi) ghost_item(g, b, 2 * n + k);
+    if (eta_hi) ghost_item(g, b, 6 * n + k);
+  }
+}
+
 // POOL: the item's descriptor is read from the constant pool (c_desc[v.desc_base + slot]);
 // otherwise from v.inst.  MODE >= 0: every instance of the batch has that mode (built for it
-// alone); -1: any mix of modes.  The finishing CTA reads the instance's full GridDev from v.inst.
-template <bool POOL, int MODE>
+// alone); -1: any mix of modes.  IG: edge items fill the ghost cells (item_ghosts), else the
+// finishing CTA fills them all; separate builds, so the item loop of the IG = false builds is
+// compiled without the ghost code.  The finishing CTA reads the instance's GridDev from v.inst.
+template <bool POOL, int MODE, bool IG>
 __global__ void __launch_bounds__(NT, POOL ? 5 : 4) batch_mixed_kernel(BatchView v) {
   __shared__ Smem S;
   __shared__ int s_item;
@@ -76,11 +128,16 @@ __global__ void __launch_bounds__(NT, POOL ? 5 : 4) batch_mixed_kernel(BatchView
           mode_item<MODE>(d, w.z, w.w, v.tile_rows, S, rows);
         else
           dispatch_item(d, d.mode, w.z, w.w, v.tile_rows, S, rows);
+        if (IG && edge_item(d.mx, d.my, w.z, w.w, v.tile_rows))
+          item_ghosts(v.inst[w.x], w.z, w.w, v.tile_rows);
       }
     } else {
       const GridDev g = v.inst[w.x];
       ctl = g.ctl;
-      if (!ctl->done) dispatch_item(g, item_mode(g), w.z, w.w, v.tile_rows, S, rows);
+      if (!ctl->done) {
+        dispatch_item(g, item_mode(g), w.z, w.w, v.tile_rows, S, rows);
+        if (IG && edge_item(g.mx, g.my, w.z, w.w, v.tile_rows)) item_ghosts(g, w.z, w.w, v.tile_rows);
+      }
     }
     int* alldone = v.counters + 2 * w.x + 1;
     __threadfence();  // every thread's writes of this item precede its completion count
@@ -95,11 +152,15 @@ __global__ void __launch_bounds__(NT, POOL ? 5 : 4) batch_mixed_kernel(BatchView
       }
     }
     __syncthreads();
-    if (s_last && ctl->ierr == 1) {  // update_rank_boundaries of the accepted instance
+    if (s_last && ctl->ierr == 1) {  // update_rank_boundaries (the rest of it after item_ghosts)
       const GridDev& g = v.inst[w.x];
       double* b = buffer(g, ctl->cur);
-      const int ng = ghost_items(g);
-      for (int k = threadIdx.x; k < ng; k += blockDim.x) ghost_item(g, b, k);
+      if (IG) {
+        finisher_ghosts(g, v.tile_rows, b);
+      } else {
+        const int ng = ghost_items(g);
+        for (int k = threadIdx.x; k < ng; k += blockDim.x) ghost_item(g, b, k);
+      }
     }
     __syncthreads();
   }
@@ -107,18 +168,23 @@ __global__ void __launch_bounds__(NT, POOL ? 5 : 4) batch_mixed_kernel(BatchView
 
 using KernelFn = void (*)(BatchView);
 
-// the build for (pool, mode); mode -1 or out of range: any mix of modes
-KernelFn kernel_for(bool pool, int mode) {
-  if (!pool) return batch_mixed_kernel<false, -1>;
+template <bool IG>
+KernelFn kernel_for_ig(bool pool, int mode) {
+  if (!pool) return batch_mixed_kernel<false, -1, IG>;
   switch (mode) {
-    case 0: return batch_mixed_kernel<true, 0>;
-    case 1: return batch_mixed_kernel<true, 1>;
-    case 2: return batch_mixed_kernel<true, 2>;
-    case 3: return batch_mixed_kernel<true, 3>;
-    case 4: return batch_mixed_kernel<true, 4>;
-    case 5: return batch_mixed_kernel<true, 5>;
-    default: return batch_mixed_kernel<true, -1>;
+    case 0: return batch_mixed_kernel<true, 0, IG>;
+    case 1: return batch_mixed_kernel<true, 1, IG>;
+    case 2: return batch_mixed_kernel<true, 2, IG>;
+    case 3: return batch_mixed_kernel<true, 3, IG>;
+    case 4: return batch_mixed_kernel<true, 4, IG>;
+    case 5: return batch_mixed_kernel<true, 5, IG>;
+    default: return batch_mixed_kernel<true, -1, IG>;
   }
+}
+
+// the build for (pool, mode, item ghosts); mode -1 or out of range: any mix of modes
+KernelFn kernel_for(bool pool, int mode, bool ig) {
+  return ig ? kernel_for_ig<true>(pool, mode) : kernel_for_ig<false>(pool, mode);
 }
 
 // pool reservations per device: used[d][k] for descriptor k
@@ -128,12 +194,12 @@ std::map<int, std::vector<char>> g_pool_used;
 }  // namespace
 
 void launch_batch_mixed(const BatchView& v, int grid, bool pool, int mode, cudaStream_t st) {
-  kernel_for(pool, mode)<<<grid, NT, 0, st>>>(v);
+  kernel_for(pool, mode, v.item_ghosts != 0)<<<grid, NT, 0, st>>>(v);
 }
 int batch_mixed_threads() { return NT; }
 int batch_mixed_occupancy(bool pool, int mode) {
-  int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_for(pool, mode), NT, 0);
+  int n = 0;  // the same for both ghost builds (same launch bounds)
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_for(pool, mode, false), NT, 0);
   return n > 0 ? n : 1;
 }
 

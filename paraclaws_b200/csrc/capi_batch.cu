@@ -81,6 +81,7 @@ struct pcl_batch {
   int tile_rows_eff = 64;  // rows per mixed item in the current items (a launch parameter)
   int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
   int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
+  int item_ghosts = 0;  // mixed: edge items fill ghost cells (few items per step), else the finisher
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   long long launches = 0;
@@ -122,6 +123,7 @@ static BatchView view(const pcl_batch* b) {
   v.y_rows = b->y_rows;
   v.tile_rows = b->tile_rows_eff;
   v.desc_base = b->desc_base;
+  v.item_ghosts = b->item_ghosts;
   v.spin_limit = 1u << 24;
   return v;
 }
@@ -225,6 +227,12 @@ static int rebuild_items(pcl_batch* b) {
     drop_graph(b);  // the captured launches point at the old item array
   }
   b->n_items = (int)items.size();
+  if (b->precision == PCL_PREC_MIXED && !items.empty()) {
+    // up to two waves of items: a step lasts a few items, so the edge items fill the ghosts
+    const int ig = (long long)items.size() <= 2LL * grid_size(b) ? 1 : 0;
+    if (ig != b->item_ghosts) drop_graph(b);  // a launch parameter of the captured launches
+    b->item_ghosts = ig;
+  }
   if (!items.empty())
     BCK(cudaMemcpyAsync(b->items_d, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaMemcpyAsync(b->totals_d, totals.data(), sizeof(int) * totals.size(), cudaMemcpyHostToDevice, b->stream));
