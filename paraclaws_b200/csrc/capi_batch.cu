@@ -139,7 +139,7 @@ static int grid_size(const pcl_batch* b) {
 
 // Rows per mixed item when the schedule leaves it open (tile_rows 0): the height that minimises
 // the estimated step time, waves x (rows an item streams + a fixed cost per item), where waves
-// is the item count over the persistent CTAs, rounded up.  A few small instances get short
+// is the item count over the persistent CTAs, rounded up, over heights 16 ... 128.  A few small instances get short
 // items spread over the SMs (a step takes about one item's time); a large batch gets taller
 // items whose four halo rows cost less.
 constexpr int kItemFixedRows = 8;
@@ -148,7 +148,9 @@ static int auto_tile_rows(const pcl_batch* b, const std::vector<int>& order) {
   const long long ctas = std::max(1, grid_size(b));
   int best = 64;
   double best_cost = 1e300;
-  for (int ty : {16, 32, 64, 128, 256}) {
+  // 256-row items are left out: their rows measured ~12% slower than 128-row items' on large
+  // grids, which the wave count does not see
+  for (int ty : {16, 32, 64, 128}) {
     long long n = 0;
     for (int s : order) {
       const auto& c = b->slots[s].cfg;
@@ -228,8 +230,14 @@ static int rebuild_items(pcl_batch* b) {
   }
   b->n_items = (int)items.size();
   if (b->precision == PCL_PREC_MIXED && !items.empty()) {
-    // up to two waves of items: a step lasts a few items, so the edge items fill the ghosts
-    const int ig = (long long)items.size() <= 2LL * grid_size(b) ? 1 : 0;
+    // The finishing CTA's ghost fill (8 max(m_xi, m_eta) cells) is hidden only behind other
+    // instances' items.  Edge items fill the ghosts instead when a step is up to two waves of
+    // items (it lasts a few items) or when one instance holds most of the items (its finisher
+    // would run at the end of the step, alone).
+    long long largest = 0;
+    for (int s : order) largest = std::max<long long>(largest, totals[2 * s + 1]);
+    const long long n = (long long)items.size();
+    const int ig = n <= 2LL * grid_size(b) || 2 * largest > n ? 1 : 0;
     if (ig != b->item_ghosts) drop_graph(b);  // a launch parameter of the captured launches
     b->item_ghosts = ig;
   }
