@@ -310,8 +310,9 @@ void* pcl_batch_get_stream(pcl_batch* batch);
    in the reference (it has no conservation diagnostics). */
 int pcl_conservation_sums(pcl_ctx* ctx, double* sums3);
 
-/* Rows per work item of the fused mixed-precision kernel (default 64; the autotuner sets it).
-   No effect on results: every cell's arithmetic is independent of the tiling. */
+/* Rows per work item of the fused mixed-precision kernel (default 128 where that still makes
+   four waves of CTAs, else 64).  No effect on results: every cell's arithmetic is independent
+   of the tiling. */
 int pcl_set_tile_rows(pcl_ctx* ctx, int rows);
 
 /* ---- one step without device allocation ---- */
