@@ -56,6 +56,11 @@ __device__ __forceinline__ void dispatch_item(const GridDev& g, int kind, int a,
   return dispatch_lim<kMetricTable>(g, kind, a, b, v, S);
 }
 
+// IG: eta items on the edge of their grid fill the ghost cells next to the cells they wrote
+// (ghost_fill_block) and the finishing CTA only the sides left open; else the finishing CTA
+// fills them all.  Separate builds, so the item loop of the IG = false build carries no ghost
+// code.  Same values either way.
+template <bool IG>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchView v) {
   __shared__ XSmem<kThreads> S;
   __shared__ int s_item;
@@ -87,7 +92,17 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
           __threadfence();
         }
         __syncthreads();
-        if (s_flag) dispatch_item(g, w.y, w.z, w.w, v, S);
+        if (s_flag) {
+          dispatch_item(g, w.y, w.z, w.w, v, S);
+          if (IG) {
+            const int i1 = min(w.z + kThreads - 1, g.mx), j1 = min(w.w + v.y_rows - 1, g.my);
+            if (w.z == 1 || w.w == 1 || i1 == g.mx || j1 == g.my) {
+              __syncthreads();  // the strip's cells, written by every thread, before any is read
+              const int cur = ctl->cur;
+              ghost_fill_block(g, buffer(g, cur == 0 ? 2 : cur - 1), w.z, i1, w.w, j1);
+            }
+          }
+        }
       } else {
         dispatch_item(g, w.y, w.z, w.w, v, S);
       }
@@ -108,8 +123,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
     __syncthreads();
     if (s_flag && ctl->ierr == 1) {  // update_rank_boundaries of the accepted instance
       double* b = buffer(g, ctl->cur);
-      const int ng = ghost_items(g);
-      for (int k = threadIdx.x; k < ng; k += blockDim.x) ghost_item(g, b, k);
+      if (IG) {
+        ghost_fill_open_sides(g, b, (g.mx - 1) % kThreads == 0, (g.my - 1) % v.y_rows == 0);
+      } else {
+        const int ng = ghost_items(g);
+        for (int k = threadIdx.x; k < ng; k += blockDim.x) ghost_item(g, b, k);
+      }
     }
     __syncthreads();
   }
@@ -118,13 +137,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
 }  // namespace
 
 void launch_batch_fp64(const BatchView& v, int grid, cudaStream_t st) {
-  batch_fp64_kernel<<<grid, kThreads, 0, st>>>(v);
+  if (v.item_ghosts)
+    batch_fp64_kernel<true><<<grid, kThreads, 0, st>>>(v);
+  else
+    batch_fp64_kernel<false><<<grid, kThreads, 0, st>>>(v);
 }
 int batch_fp64_threads() { return kThreads; }
 int batch_fp64_segment() { return kThreads - 4; }
 int batch_fp64_occupancy() {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_fp64_kernel, kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_fp64_kernel<false>, kThreads, 0);
   return n > 0 ? n : 1;
 }
 

@@ -51,52 +51,25 @@ __device__ __forceinline__ int item_mode(const GridDev& g) { return g.second_ord
 
 // Ghost cells (update_rank_boundaries) filled by the items themselves, when the batch is small
 // enough that its step time is a few items' latency (the IG builds; with many items the
-// finishing CTA's fill overlaps other CTAs' items and costs less).  Same values either way.  A ghost value reads
-// interior cells within two cells of its side, of the buffer the step writes.  An item that
-// wrote those cells fills that side's ghosts along its own rows (xi sides) or columns (eta
-// sides) once its rows are done, before its completion count.  They go into the step's output
-// buffer whether or not the step is then accepted: a rejected step leaves that buffer unused.
-// Only the high side of a grid whose last strip (segment) is one column (row) wide has its two
-// source cells in different items; the finishing CTA fills that one (finisher_ghosts).
+// finishing CTA's fill overlaps other CTAs' items and costs less).  Same values either way:
+// an edge item fills the ghosts next to the cells it wrote (ghost_fill_block), into the step's
+// output buffer, before its completion count.
 __device__ __forceinline__ void item_ghosts(const GridDev& g, int strip, int seg, int ty) {
-  const int mx = g.mx, my = g.my, n = max(mx, my);
   const int cur = g.ctl->cur;
-  double* b = buffer(g, cur == 0 ? 2 : cur - 1);
-  const int i0 = 1 + strip * mixed::TXI, i1 = min(i0 + mixed::TXI - 1, mx);
-  const int j0 = 1 + seg * ty, j1 = min(j0 + ty - 1, my);
-  const int nc = i1 - i0 + 1, nr = j1 - j0 + 1;
-  const int c0 = strip == 0 ? 2 * nr : 0;                // xi low: sources i = 1, 2
-  const int c1 = i1 == mx && nc >= 2 ? 2 * nr : 0;       // xi high: i = mx, mx - 1
-  const int c2 = seg == 0 ? 2 * nc : 0;                  // eta low: j = 1, 2
-  const int c3 = j1 == my && nr >= 2 ? 2 * nc : 0;       // eta high: j = my, my - 1
-  const int total = c0 + c1 + c2 + c3;
-  for (int k = threadIdx.x; k < total; k += blockDim.x) {
-    int side = 0, r = k;
-    if (r >= c0) { r -= c0; side = 1;
-      if (r >= c1) { r -= c1; side = 2;
-        if (r >= c2) { r -= c2; side = 3; } } }
-    const int len = side < 2 ? nr : nc;
-    const int layer = r / len;
-    const int pos = (side < 2 ? j0 : i0) + (r - layer * len);  // 1-based along the side
-    ghost_item(g, b, side * 2 * n + layer * n + (pos - 1));
-  }
+  const int i0 = 1 + strip * mixed::TXI, j0 = 1 + seg * ty;
+  ghost_fill_block(g, buffer(g, cur == 0 ? 2 : cur - 1), i0, min(i0 + mixed::TXI - 1, g.mx), j0,
+                   min(j0 + ty - 1, g.my));
+}
+
+// The sides item_ghosts leaves open, after an accepted step (b: the new current buffer).
+__device__ __forceinline__ void finisher_ghosts(const GridDev& g, int ty, double* b) {
+  ghost_fill_open_sides(g, b, (g.mx - 1) % mixed::TXI == 0, (g.my - 1) % ty == 0);
 }
 
 // True for an item on the edge of its grid (first or last strip or segment): only those write
 // ghost cells, and the rest skip item_ghosts without reading the grid's descriptor.
 __device__ __forceinline__ bool edge_item(int mx, int my, int strip, int seg, int ty) {
   return strip == 0 || seg == 0 || (strip + 1) * mixed::TXI >= mx || (seg + 1) * ty >= my;
-}
-
-// The sides item_ghosts leaves open, after an accepted step (b: the new current buffer).
-__device__ __forceinline__ void finisher_ghosts(const GridDev& g, int ty, double* b) {
-  const int n = max(g.mx, g.my);
-  const bool xi_hi = (g.mx - 1) % mixed::TXI == 0;  // last strip one column wide
-  const bool eta_hi = (g.my - 1) % ty == 0;         // last segment one row high
-  for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) {
-    if (xi_hi) ghost_item(g, b, 2 * n + k);
-    if (eta_hi) ghost_item(g, b, 6 * n + k);
-  }
 }
 
 // POOL: the item's descriptor is read from the constant pool (c_desc[v.desc_base + slot]);

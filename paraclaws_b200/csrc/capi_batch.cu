@@ -81,7 +81,7 @@ struct pcl_batch {
   int tile_rows_eff = 64;  // rows per mixed item in the current items (a launch parameter)
   int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
   int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
-  int item_ghosts = 0;  // mixed: edge items fill ghost cells (few items per step), else the finisher
+  int item_ghosts = 0;  // edge items fill ghost cells (few items per step), else the finisher does
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   long long launches = 0;
@@ -229,7 +229,7 @@ static int rebuild_items(pcl_batch* b) {
     drop_graph(b);  // the captured launches point at the old item array
   }
   b->n_items = (int)items.size();
-  if (b->precision == PCL_PREC_MIXED && !items.empty()) {
+  if (!items.empty()) {
     // The finishing CTA's ghost fill (8 max(m_xi, m_eta) cells) is hidden only behind other
     // instances' items.  Edge items fill the ghosts instead when a step is up to two waves of
     // items (it lasts a few items) or when one instance holds most of the items (its finisher

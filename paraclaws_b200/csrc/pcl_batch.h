@@ -42,8 +42,8 @@ struct BatchView {
   int y_rows;            // rows per FP64 eta strip
   int tile_rows;         // rows per mixed item
   int desc_base;         // first pool descriptor of this batch (mixed, pool build only)
-  int item_ghosts;       // mixed: 1 = the build whose edge items fill ghost cells, 0 = the
-                         // build whose finishing CTA fills them all
+  int item_ghosts;       // 1: the builds whose edge items fill ghost cells, 0: the builds
+                         // whose finishing CTA fills them all
   unsigned spin_limit;   // bounded waits of eta items for their xi items
 };
 

@@ -106,4 +106,49 @@ __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid)
   if (ghost_value(g, b, tid, o)) ghost_store(g, o);
 }
 
+// Ghost cells next to a block of interior cells [i0, i1] x [j0, j1] of buffer b that the calling
+// CTA has just written (batched kernels, before the step's accept decision: a rejected step
+// leaves b unused).  A ghost value reads interior cells within two cells of its side, so the
+// block fills a side along its own rows (xi) or columns (eta) when it holds both source cells:
+// always on the low sides (cells 1 and 2 lie in the first block of a grid at least two cells
+// wide), on a high side when the block is at least two cells deep there.  All threads of the CTA.
+__device__ __forceinline__ void ghost_fill_block(const GridDev& g, double* b, int i0, int i1, int j0, int j1) {
+  const int mx = g.mx, my = g.my, n = max(mx, my);
+  const int nc = i1 - i0 + 1, nr = j1 - j0 + 1;
+  const int c0 = i0 == 1 ? 2 * nr : 0;               // xi low: sources i = 1, 2
+  const int c1 = i1 == mx && nc >= 2 ? 2 * nr : 0;   // xi high: i = mx, mx - 1
+  const int c2 = j0 == 1 ? 2 * nc : 0;               // eta low: j = 1, 2
+  const int c3 = j1 == my && nr >= 2 ? 2 * nc : 0;   // eta high: j = my, my - 1
+  const int total = c0 + c1 + c2 + c3;
+  for (int k = threadIdx.x; k < total; k += blockDim.x) {
+    int side = 0, r = k;
+    if (r >= c0) {
+      r -= c0;
+      side = 1;
+      if (r >= c1) {
+        r -= c1;
+        side = 2;
+        if (r >= c2) {
+          r -= c2;
+          side = 3;
+        }
+      }
+    }
+    const int len = side < 2 ? nr : nc;
+    const int layer = r / len;
+    const int pos = (side < 2 ? j0 : i0) + (r - layer * len);  // 1-based along the side
+    ghost_item(g, b, side * 2 * n + layer * n + (pos - 1));
+  }
+}
+
+// The high sides ghost_fill_block leaves to whoever runs after all blocks: xi high when the last
+// block column is one cell wide, eta high when the last block row is one cell deep.
+__device__ __forceinline__ void ghost_fill_open_sides(const GridDev& g, double* b, bool xi_hi, bool eta_hi) {
+  const int n = max(g.mx, g.my);
+  for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) {
+    if (xi_hi) ghost_item(g, b, 2 * n + k);
+    if (eta_hi) ghost_item(g, b, 6 * n + k);
+  }
+}
+
 }  // namespace pcl

@@ -154,23 +154,25 @@ def test_single_mode_builds_and_switch_to_mixed_modes(pcl, first_mode):
     b.close()
 
 
-@pytest.mark.parametrize("tile_rows", [16, 32, 0])
-def test_item_ghost_fill_matches_alone(pcl, tile_rows):
-    """Mixed items fill the ghost cells next to the cells they wrote; the finishing CTA fills a
-    high side whose last strip (segment) is one column (row) wide.  Grids with m_xi = 1 or 2 past
-    a multiple of the 124-column strip and m_eta = 1 or 2 past a multiple of the tile height,
-    each side with its own boundary code, end bit-identical to running alone, ghost cells
-    included."""
-    shapes = [(125, 33), (249, 17), (126, 65), (131, 97), (248, 34)]
-    codes = [(1, 3, 2, 3), (3, 1, 3, 2), (2, 2, 1, 1), (3, 3, 3, 3), (1, 2, 3, 1)]
+@pytest.mark.parametrize("precision,rows", [(ctl.PRECISION_MIXED, 16), (ctl.PRECISION_MIXED, 32),
+                                            (ctl.PRECISION_MIXED, 0), (ctl.PRECISION_FP64, 16),
+                                            (ctl.PRECISION_FP64, 32)])
+def test_item_ghost_fill_matches_alone(pcl, precision, rows):
+    """Edge items fill the ghost cells next to the cells they wrote; the finishing CTA fills a
+    high side whose last strip (segment) is one column (row) wide.  Grids with m_xi one or two past
+    a multiple of the strip width (124 columns mixed, 128 FP64) and m_eta one or two past a
+    multiple of the item height (`rows`: mixed tile rows, FP64 eta strip rows), each side with its
+    own boundary code, end bit-identical to running alone, ghost cells included."""
+    shapes = [(125, 33), (249, 17), (129, 65), (257, 97), (248, 34), (126, 66)]
+    codes = [(1, 3, 2, 3), (3, 1, 3, 2), (2, 2, 1, 1), (3, 3, 3, 3), (1, 2, 3, 1), (3, 2, 1, 3)]
     cases = []
     for k, ((mx, my), (b0, b1, b2, b3)) in enumerate(zip(shapes, codes)):
         c = dataclasses.replace(ctl.dam_break_control(mx, limiter=1 + k % 4, bc=1, time_final=0.03), m_eta=my,
                                 bc_xi_lower=b0, bc_xi_upper=b1, bc_eta_lower=b2, bc_eta_upper=b3)
         p = ic.seeded_dam_params(k, offset=0.25)
         cases.append((c, ic.circular_dam(mx, my, p.radius, p.h_in, p.h_out, p.x0, p.y0)))
-    b = Batch(8, precision=ctl.PRECISION_MIXED)
-    b.set_schedule(Schedule(tile_rows=tile_rows))
+    b = Batch(8, precision=precision)
+    b.set_schedule(Schedule(tile_rows=rows) if precision == ctl.PRECISION_MIXED else Schedule(x_rows=4, y_rows=rows))
     slots = [b.add(c, q) for c, q in cases]
     for _ in range(400):
         b.step(16)
@@ -178,15 +180,16 @@ def test_item_ghost_fill_matches_alone(pcl, tile_rows):
         if all(done[s] == 1 for s in slots):
             break
     for s, (c, q) in zip(slots, cases):
-        qa, la = _alone(c, q, ctl.PRECISION_MIXED)
+        qa, la = _alone(c, q, precision)
         assert np.array_equal(b.step_log(s).dt, la.dt)
         assert np.array_equal(b.download(s), qa)
     b.close()
 
 
-def test_ghost_fill_by_finishing_cta_matches_alone(pcl):
-    """With many items per step (here 4-row items on one CTA per SM) the finishing CTA fills all
-    ghost cells instead of the edge items; the grids still end bit-identical to running alone."""
+@pytest.mark.parametrize("precision", [ctl.PRECISION_MIXED, ctl.PRECISION_FP64])
+def test_ghost_fill_by_finishing_cta_matches_alone(pcl, precision):
+    """With many items per step (short items on one CTA per SM) the finishing CTA fills all ghost
+    cells instead of the edge items; the grids still end bit-identical to running alone."""
     shapes = [(260, 260), (249, 257), (300, 201)]
     codes = [(1, 3, 2, 3), (3, 1, 3, 1), (2, 3, 1, 2)]
     cases = []
@@ -195,8 +198,9 @@ def test_ghost_fill_by_finishing_cta_matches_alone(pcl):
                                 bc_xi_lower=b0, bc_xi_upper=b1, bc_eta_lower=b2, bc_eta_upper=b3)
         p = ic.seeded_dam_params(k + 20, offset=0.25)
         cases.append((c, ic.circular_dam(mx, my, p.radius, p.h_in, p.h_out, p.x0, p.y0)))
-    b = Batch(4, precision=ctl.PRECISION_MIXED)
-    b.set_schedule(Schedule(tile_rows=4, blocks_per_sm=1))
+    b = Batch(4, precision=precision)
+    b.set_schedule(Schedule(tile_rows=4, blocks_per_sm=1) if precision == ctl.PRECISION_MIXED
+                   else Schedule(x_rows=1, y_rows=4, blocks_per_sm=1))
     slots = [b.add(c, q) for c, q in cases]
     for _ in range(400):
         b.step(16)
@@ -204,7 +208,7 @@ def test_ghost_fill_by_finishing_cta_matches_alone(pcl):
         if all(done[s] == 1 for s in slots):
             break
     for s, (c, q) in zip(slots, cases):
-        qa, la = _alone(c, q, ctl.PRECISION_MIXED)
+        qa, la = _alone(c, q, precision)
         assert np.array_equal(b.step_log(s).dt, la.dt)
         assert np.array_equal(b.download(s), qa)
     b.close()
