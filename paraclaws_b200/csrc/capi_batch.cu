@@ -82,6 +82,7 @@ struct pcl_batch {
   int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
   int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
   int item_ghosts = 0;  // edge items fill ghost cells (few items per step), else the finisher does
+  int launch_ctas = 0;  // CTAs per launch: the persistent grid, or fewer when there are fewer items
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   long long launches = 0;
@@ -240,6 +241,10 @@ static int rebuild_items(pcl_batch* b) {
     const int ig = n <= 2LL * grid_size(b) || 2 * largest > n ? 1 : 0;
     if (ig != b->item_ghosts) drop_graph(b);  // a launch parameter of the captured launches
     b->item_ghosts = ig;
+    // a CTA without an item only sets up its ring and leaves: launch no more CTAs than items
+    const int ctas = (int)std::min<long long>(grid_size(b), n);
+    if (ctas != b->launch_ctas) drop_graph(b);
+    b->launch_ctas = ctas;
   }
   if (!items.empty())
     BCK(cudaMemcpyAsync(b->items_d, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, b->stream));
@@ -255,9 +260,9 @@ static void enqueue_step(pcl_batch* b) {
   cudaMemsetAsync(b->scal_d + 1, 0, sizeof(int), b->stream);
   const BatchView v = view(b);
   if (b->precision == PCL_PREC_MIXED)
-    launch_batch_mixed(v, grid_size(b), b->desc_base >= 0, b->mode, b->stream);
+    launch_batch_mixed(v, b->launch_ctas, b->desc_base >= 0, b->mode, b->stream);
   else
-    launch_batch_fp64(v, grid_size(b), b->stream);
+    launch_batch_fp64(v, b->launch_ctas, b->stream);
 }
 
 extern "C" {
