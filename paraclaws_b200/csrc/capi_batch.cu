@@ -140,7 +140,7 @@ static int grid_size(const pcl_batch* b) {
 
 // Rows per mixed item when the schedule leaves it open (tile_rows 0): the height that minimises
 // the estimated step time, waves x (rows an item streams + a fixed cost per item), where waves
-// is the item count over the persistent CTAs, rounded up, over heights 16 ... 128.  A few small instances get short
+// is the item count over the persistent CTAs, rounded up, over heights 8 ... 128.  A few small instances get short
 // items spread over the SMs (a step takes about one item's time); a large batch gets taller
 // items whose four halo rows cost less.
 constexpr int kItemFixedRows = 8;
@@ -151,7 +151,7 @@ static int auto_tile_rows(const pcl_batch* b, const std::vector<int>& order) {
   double best_cost = 1e300;
   // 256-row items are left out: their rows measured ~12% slower than 128-row items' on large
   // grids, which the wave count does not see
-  for (int ty : {16, 32, 64, 128}) {
+  for (int ty : {8, 16, 32, 64, 128}) {
     long long n = 0;
     for (int s : order) {
       const auto& c = b->slots[s].cfg;

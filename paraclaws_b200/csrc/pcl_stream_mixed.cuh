@@ -4,7 +4,7 @@
 //
 // Work item: a strip of TXI = 124 columns x a segment of TY rows.  The CTA streams the rows
 // j0-2 .. j1+2 of its strip (plus two halo columns each side) through a four-slot shared-memory
-// ring filled by bulk copies (cp.async.bulk, completion on an mbarrier), two rows ahead.  For each
+// ring filled by bulk copies (cp.async.bulk, completion on an mbarrier), three rows ahead.  For each
 // row: the xi sweep of that row runs in shared memory (per-cell flux data, HLL per interface,
 // limited correction flux, update); thread t keeps the x-swept FP64 value of its own column
 // i0+t in registers and advances its eta-sweep register window (interfaces j-2 .. j) by one
@@ -34,7 +34,7 @@ namespace mixed {
 constexpr int NT = 128;      // threads per CTA = slots of a streamed row
 constexpr int TXI = NT - 4;  // interior columns of a strip
 constexpr int RING = 4;      // row slots
-constexpr int AHEAD = 2;     // rows in flight ahead of the one being processed
+constexpr int AHEAD = 3;     // rows in flight ahead of the one being processed
 constexpr float kEps = 1e-10f;
 
 struct CellM {
@@ -329,7 +329,7 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
       }
       cprev = cn;
     }
-    __syncthreads();  // slot k&3 is refilled two rows from now
+    __syncthreads();  // this row's slot is refilled at the start of the next row
   }
 
   if (timed_out && t == 0) {
