@@ -39,12 +39,12 @@ extern "C" {
 #define PCL_PREC_MIXED 1  /* FP32 flux/limiter arithmetic, FP64 state, FP64 dt and sums */
 
 /* boundary-condition codes (user_subroutines/SMOD_boundary_conditions.f90:13) */
-#define PCL_BC_WALL 1          /* BC_USER slot: reflective wall in this build */
+#define PCL_BC_WALL 1          /* BC_USER slot: reflective wall in this library */
 #define PCL_BC_ZERO_GRADIENT 2
 #define PCL_BC_CONST_GRADIENT 3
 
 /* Everything read_solver_control reads from control.in (utility/MOD_IO.f90:61-94), in that
-   order, plus the settings this build reads from custom.in (the reference leaves custom.in
+   order, plus the settings this library reads from custom.in (the reference leaves custom.in
    unread: custom_settings.py:16-22). */
 typedef struct pcl_solver_control {
   int num_equations, num_dimensions, num_ghost, num_aux, num_waves;
@@ -87,7 +87,8 @@ typedef struct pcl_step_record {
 void pcl_default_control(pcl_solver_control* out);
 
 /* Parse control.in (28 list-directed records, utility/MOD_IO.f90:55-94) and, if custom_in is
-   not NULL and exists, this build's custom.in.  Replaces read_solver_control's reads. */
+   not NULL and exists, custom.in as this library defines it.  Replaces read_solver_control's
+   reads. */
 int pcl_read_solver_control(const char* control_in, const char* custom_in, pcl_solver_control* out);
 
 /* ---- context lifecycle ---- */
@@ -151,7 +152,7 @@ typedef struct pcl_device_view {
 typedef pcl_device_view pcl_bc_view;
 
 /* The reference leaves BC_USER unimplemented (it aborts, SMOD_boundary_conditions.f90:83-211);
-   this build fills it with a reflective wall unless a hook is set.  The hook enqueues the
+   this library fills it with a reflective wall unless a hook is set.  The hook enqueues the
    caller's own device work on `stream` (a cudaStream_t) for the sides in `sides` (bit 0 xi low,
    1 xi high, 2 eta low, 3 eta high: those coded 1) and returns 0, or nonzero on failure
    (PCL_ERR_USER).  It must only enqueue: the library calls it wherever it fills ghosts, also

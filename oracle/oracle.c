@@ -640,7 +640,7 @@ int orc_solve_dimensional_split(orc_t* o, int* ierr)
 
 /* ------------------------------------------------------------------------------------- */
 /* Boundary conditions: user_subroutines/SMOD_boundary_conditions.f90:58-213              */
-/* code 1 (BC_USER; the reference aborts) is filled in this build with a reflective wall:  */
+/* code 1 (BC_USER; the reference aborts) is filled here with a reflective wall:  */
 /* mirror the two nearest interior cells and negate the normal momentum.                   */
 /* ------------------------------------------------------------------------------------- */
 static double deriv_2p(double x1, double x2, double y1, double y2) { return (y2 - y1) / (x2 - x1); }

@@ -8,7 +8,7 @@ reads of ``utility/MOD_IO.f90:55-94``: the first value of each record, in order,
 logical and ``d``-exponent syntax accepted.
 
 ``custom.in`` is written but never read by the reference (its ``FIELD_ORDER`` is empty,
-``custom_settings.py:16-22``); this build uses it, positionally as well, for the settings the
+``custom_settings.py:16-22``); this library uses it, positionally as well, for the settings the
 reference has no slot for (``CustomSettings``).
 """
 from __future__ import annotations
@@ -98,7 +98,7 @@ PRECISION_MIXED = 1
 
 @dataclass
 class CustomSettings:
-    """custom.in for this build (positional, one value per line, like control.in)."""
+    """custom.in as this library reads it (positional, one value per line, like control.in)."""
 
     max_accepted_steps: int = 0          # 0: run to time_final only
     precision_mode: int = PRECISION_FP64
