@@ -21,6 +21,7 @@ from typing import Deque, Dict, List, Optional
 
 import numpy as np
 
+from ._lib import PCL_ERR_FULL
 from .batch import Batch, autotune
 from .control import ControlSettings, CustomSettings, PRECISION_FP64, dam_break_control
 from . import ic
@@ -150,8 +151,18 @@ class SolveServer:
             while i < len(pending) and pending[i].arrival <= now:
                 arrived.append(pending[i])
                 i += 1
-            # admit in arrival order while memory and slots allow (no overtaking)
-            while arrived and self._admit(arrived[0], clock() - t0):
+            # admit in arrival order while memory and slots allow (no overtaking).  A request larger
+            # than the whole budget could never be admitted and would hold up every request behind
+            # it: it is answered at once with PCL_ERR_FULL.
+            while arrived:
+                r = arrived[0]
+                if self.footprint(r) > self.budget:
+                    arrived.popleft()
+                    t = clock() - t0
+                    results.append(Result(r.rid, r.arrival, t, t, 0, r.control.m_xi * r.control.m_eta, PCL_ERR_FULL))
+                    continue
+                if not self._admit(r, clock() - t0):
+                    break
                 arrived.popleft()
             peak_bytes = max(peak_bytes, self.in_use)
             peak_active = max(peak_active, len(self.active))
