@@ -35,8 +35,9 @@ BYTES_PER_CELL_UPDATE = 96         # two sweeps
 
 
 def workload(m: int):
+    """C2's settings: minmod, reflective walls on all four sides, CFL 0.9, dt_max 1e-2."""
     from paraclaws_b200 import control as ctl
-    c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=1.0e9)
+    c = ctl.dam_break_control(m, limiter=1, bc=1, time_final=1.0e9)
     return c
 
 
@@ -217,8 +218,8 @@ def aggregate_over_ranks(dist, ms: float, accepted: int, device) -> tuple:
 
 def config_dict(args) -> dict:
     return {"workload": f"plain-large: {args.grid}^2 dam-break grid, 16 seeded Gaussian bumps (seed 0), "
-                        f"minmod-limited second-order HLL, CFL 0.9, {args.steps} accepted steps",
-            "grid": args.grid, "precision": args.precision, "limiter": "minmod", "bc": "zero-gradient",
+                        f"minmod-limited second-order HLL, reflective walls, CFL 0.9, {args.steps} accepted steps",
+            "grid": args.grid, "precision": args.precision, "limiter": "minmod", "bc": "reflective walls",
             "l2": "inputs larger than L2 (state buffer %.0f MB > 126 MB)" % (3 * 8 * (args.grid + 4) ** 2 / 1e6),
             "parallelism": "replicas" if args.gpus > 1 else "single"}
 
@@ -321,7 +322,7 @@ def form_snapshots(device, m=1024, time_final=0.05, snapshots=5):
 
     from paraclaws_b200 import control as ctl
     from paraclaws_b200.solver import Solver, run_device_loop_with_snapshots
-    c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=time_final)
+    c = ctl.dam_break_control(m, limiter=1, bc=1, time_final=time_final)
     c.number_of_snapshots = snapshots
     out = {}
     for mode in ("plain", "snapshots"):
@@ -407,7 +408,7 @@ def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 30
     names = ("h", "hu", "hv")
 
     def run(cfl, cps):
-        c = ctl.dam_break_control(m, limiter=1, bc=2, time_final=1.0e9, cfl=cfl)
+        c = ctl.dam_break_control(m, limiter=1, bc=1, time_final=1.0e9, cfl=cfl)
         runs = {"fp64": (ctl.PRECISION_FP64, q), "mixed": (ctl.PRECISION_MIXED, q),
                 "fp64_perturbed": (ctl.PRECISION_FP64, qp)}
         solvers, sums0 = {}, {}
@@ -462,42 +463,119 @@ def form_precision(device, m=8192, steps=1000, seed=1, checkpoints=(100, 200, 30
     return out
 
 
-def form_batch(device, n=512, steps=32, precisions=("fp64", "mixed")):
-    """512 dam-break instances, sides log-uniform 64..1024 (multiples of 32), own dt each."""
-    import torch
+def batch_instances(n: int = 512, seed: int = 2):
+    """C4's instances: sides log-uniform 64 .. 1024 in multiples of 32 (seed 2), seeded dams
+    (radius, height ratio, centre offset within 0.25), minmod, reflective walls, CFL 0.9."""
+    from paraclaws_b200 import ic
+    sides = ic.log_uniform_sides(n, 64, 1024, 32, seed=seed)
+    return sides, [ic.seeded_dam_params(k, offset=0.25) for k in range(n)]
+
+
+def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None):
+    """One batch of the C4 instances, each stopping after `accepted_steps` accepted steps.  With
+    perturb_seed, the FP64 start has h raised by one ulp in 1% of the cells (host-built state)."""
+    import numpy as np
 
     from paraclaws_b200 import control as ctl
     from paraclaws_b200 import ic
-    from paraclaws_b200.batch import Batch, autotune
-    sides = ic.log_uniform_sides(n, 64, 1024, 32, seed=2)
+    from paraclaws_b200.batch import Batch
+    b = Batch(len(sides), precision=prec, device=device)
+    rng = np.random.Generator(np.random.PCG64(perturb_seed)) if perturb_seed is not None else None
+    for m, p in zip(sides, params):
+        cu = ctl.CustomSettings(precision_mode=prec, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out,
+                                dam_x0=p.x0, dam_y0=p.y0, max_accepted_steps=accepted_steps)
+        q = None
+        if rng is not None:
+            q = ic.circular_dam(m, m, p.radius, p.h_in, p.h_out, p.x0, p.y0)
+            mask = rng.random(q.shape[:2]) < 0.01
+            q[..., 0] = np.where(mask, np.nextafter(q[..., 0], np.inf), q[..., 0])
+        b.add(ctl.dam_break_control(m, limiter=1, bc=1, time_final=1.0e9), q, cu)
+    return b
+
+
+def _run_to_completion(b, torch):
+    """Step every instance to its accepted-step cap; CUDA events on the batch stream around the
+    whole loop (the host's done polls between graph launches included)."""
+    stream = torch.cuda.ExternalStream(b.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    attempts = 0
+    e0.record(stream)
+    while True:
+        b.step(16)
+        attempts += 16
+        done, _ = b.poll()
+        if (done[done >= 0] == 1).all():
+            break
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1), attempts
+
+
+def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), l1=True):
+    """C4: 512 dam-break instances, each with its own adaptive dt, run to 200 accepted steps each
+    in one persistent launch per attempted step (CUDA graphs of 16), after the autotuner picked
+    the schedule on a separate copy of the batch.  Work = sum over instances of m^2 x accepted
+    steps (rejected attempts count as time only).  Then L1(h) of every mixed instance against the
+    same instance in FP64, beside the FP64 conditioning floor (FP64 from a start with h + 1 ulp
+    in 1% of the cells)."""
+    import numpy as np
+    import torch
+
+    from paraclaws_b200 import control as ctl
+    from paraclaws_b200.batch import autotune
+    sides, params = batch_instances(n)
+    peak, _ = hbm_peak()
     res = {}
+    finals = {}
     for name, prec in (("fp64", ctl.PRECISION_FP64), ("mixed", ctl.PRECISION_MIXED)):
         if name not in precisions:
             continue
-        b = Batch(n, precision=prec, device=device)
-        for k, m in enumerate(sides):
-            p = ic.seeded_dam_params(k, offset=0.25)
-            cu = ctl.CustomSettings(precision_mode=prec, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out,
-                                    dam_x0=p.x0, dam_y0=p.y0)
-            b.add(ctl.dam_break_control(m, limiter=1, time_final=1.0e9), None, cu)
-        best, _ = autotune(b, steps_per_trial=4, use_cache=False)
-        stream = torch.cuda.ExternalStream(b.stream)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        b.step(steps)
-        e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        cells = sum(m * m for m in sides)
-        peak, _ = hbm_peak()
-        v = cells / (ms * 1e-3)
-        res[name] = {"value": v, "unit": UNIT, "ms_per_step": ms, "schedule": best.__dict__,
+        tb = _make_batch(prec, sides, params, device, 0)
+        best, _ = autotune(tb, steps_per_trial=4, use_cache=False)
+        tb.close()
+        b = _make_batch(prec, sides, params, device, accepted_steps)
+        b.set_schedule(best)
+        ms, attempts = _run_to_completion(b, torch)
+        acc = np.array([b.stats(k).accepted for k in range(n)])
+        att = np.array([b.stats(k).attempts for k in range(n)])
+        cell_updates = float(sum(m * m * int(a) for m, a in zip(sides, acc)))
+        v = cell_updates / (ms * 1e-3)
+        res[name] = {"value": v, "unit": UNIT, "wall_ms": ms, "accepted_per_instance": [int(acc.min()), int(acc.max())],
+                     "attempts_per_instance": [int(att.min()), int(att.max())], "launches": attempts,
+                     "ms_per_launch": ms / attempts, "schedule": best.__dict__,
                      "effective_roofline_frac": v * BYTES_PER_CELL_UPDATE / 1e9 / peak}
+        if name == "mixed":
+            res[name]["dram_roofline_frac"] = v * BYTES_PER_CELL_SWEEP / 1e9 / peak
+            res[name]["note"] = ("fused kernel: 48 B of DRAM traffic per cell-update (dram_roofline_frac); "
+                                 "effective_roofline_frac scores it against the two-sweep step's 96 B")
+        if l1:
+            finals[name] = b
+        else:
+            b.close()
+    if l1 and len(finals) == 2:
+        fb = _make_batch(ctl.PRECISION_FP64, sides, params, device, accepted_steps, perturb_seed=7)
+        _run_to_completion(fb, torch)
+        l1_mixed, l1_floor = [], []
+        for k in range(n):
+            ref = finals["fp64"].download(k)[2:-2, 2:-2, 0]
+            scale = float(np.abs(ref).sum())
+            l1_mixed.append(float(np.abs(finals["mixed"].download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
+            l1_floor.append(float(np.abs(fb.download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
+        fb.close()
+        worst = int(np.argmax(l1_mixed))
+        res["l1_h_mixed_vs_fp64"] = {"median": float(np.median(l1_mixed)), "p99": float(np.percentile(l1_mixed, 99)),
+                                     "max": float(max(l1_mixed)), "max_instance_side": int(sides[worst]),
+                                     "instances": n, "accepted_steps": accepted_steps}
+        res["l1_h_fp64_floor"] = {"median": float(np.median(l1_floor)), "max": float(max(l1_floor)),
+                                  "note": "FP64 vs FP64 from the same start with h + 1 ulp in 1% of the cells"}
+    for b in finals.values():
         b.close()
     res["instances"] = n
-    res["cells"] = sum(m * m for m in sides)
+    res["cells"] = int(sum(m * m for m in sides))
     res["launches_per_step"] = 1
+    res["workload"] = (f"C4: {n} dam breaks, sides log-uniform 64..1024 (multiples of 32, seed 2), seeded dams, "
+                       f"minmod, walls, CFL 0.9, {accepted_steps} accepted steps each")
     return res
 
 
@@ -553,6 +631,41 @@ def form_serving(device, l1_sample: int = 8):
                                                   "+1 ulp in 1% of the cells (the step's own amplification)"}
         res[name].append(entry)
     return res
+
+def _sig(x, digits=4):
+    return float(f"{x:.{digits}g}") if isinstance(x, float) else x
+
+
+def target_summary(fp64_value: float, forms: dict) -> dict:
+    """The north-star target, compact: the mixed-precision batched form (C4, accepted-step work)
+    against the plain FP64 path (this line's value), its roofline fractions, its L1(h) against
+    the FP64 batch, and the serving latencies of both precisions."""
+    b = forms.get("batch", {})
+    mx = b.get("mixed", {})
+    l1 = b.get("l1_h_mixed_vs_fp64", {})
+    fl = b.get("l1_h_fp64_floor", {})
+    srv = forms.get("serving", {})
+
+    def serve(name, rate):
+        for e in srv.get(name, []):
+            if e.get("rate_per_s") == rate:
+                return {"rate_per_s": rate, "p50_s": _sig(e["p50_s"]), "p99_s": _sig(e["p99_s"])}
+        return None
+
+    v = mx.get("value")
+    t = {"mixed_batch_cell_updates_per_s": _sig(v), "plain_fp64_cell_updates_per_s": _sig(fp64_value),
+         "speedup_vs_fp64": _sig(v / fp64_value) if v else None,
+         "effective_roofline_frac": _sig(mx.get("effective_roofline_frac")),
+         "dram_roofline_frac": _sig(mx.get("dram_roofline_frac")),
+         "l1_h_mixed_vs_fp64_median": _sig(l1.get("median")), "l1_h_mixed_vs_fp64_max": _sig(l1.get("max")),
+         "l1_h_fp64_floor_median": _sig(fl.get("median")),
+         "serving_mixed": serve("mixed", 12.0), "serving_fp64": serve("fp64", 3.0),
+         "workload": "C4, 512 instances x 200 accepted steps; serving C5"}
+    if v:
+        t["met"] = {"speedup_ge_2": v / fp64_value >= 2.0, "effective_roofline_ge_0.70": mx["effective_roofline_frac"] >= 0.7,
+                    "l1_h_max_le_1e-5": bool(l1) and l1["max"] <= 1e-5}
+    return t
+
 
 # ------------------------------------------------------------------------------------------
 # our arm
@@ -704,13 +817,16 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(m)
     if rank == 0 and world == 1 and not args.no_forms:
-        line["forms"] = {"mixed": form_mixed(m, args.steps, args.warmup, local, value),
-                         "mapped": form_mapped(m, min(args.steps, 200), args.warmup, local, value),
-                         "snapshots": form_snapshots(local),
-                         "equations": form_equations(m, min(args.steps, 200), args.warmup, local, value),
-                         "batch": form_batch(local),
-                         "serving": form_serving(local),
-                         "precision": form_precision(local)}
+        forms = {"mixed": form_mixed(m, args.steps, args.warmup, local, value),
+                 "mapped": form_mapped(m, min(args.steps, 200), args.warmup, local, value),
+                 "snapshots": form_snapshots(local),
+                 "equations": form_equations(m, min(args.steps, 200), args.warmup, local, value),
+                 "batch": form_batch(local),
+                 "serving": form_serving(local),
+                 "precision": form_precision(local)}
+        line["forms"] = forms
+        # last key of the line: the north-star target on its own stated terms
+        line["target"] = target_summary(value, forms)
     s.close()
     if dist is not None:
         dist.barrier()

@@ -136,8 +136,8 @@ int pcl_format_e26_16(double value, char* out);
 /* What a device hook (user boundary condition, source term) sees: the context's device state,
    the current-buffer index and the attempt's flags. */
 typedef struct pcl_device_view {
-  double* state;               /* device: rotation buffer b, plane p (0 h, 1 hu, 2 hv) at
-                                  state + b*buffer_stride + p*plane_stride */
+  double* state;               /* device: rotation buffer b, plane p (shallow water: 0 h, 1 hu,
+                                  2 hv) at state + b*buffer_stride + p*plane_stride */
   long long buffer_stride;     /* doubles */
   long long plane_stride;      /* doubles */
   int pitch;                   /* doubles per row: cell (i, j), i, j = -1 .. m+2, at (j+1)*pitch + (i+1) */
@@ -148,6 +148,7 @@ typedef struct pcl_device_view {
   const int* current_buffer;   /* device int: index of the buffer holding the current solution */
   const int* attempt_accepted; /* device int: 1 when the attempt just taken was accepted */
   const double* step_dt;       /* device double: dt of that attempt */
+  int num_equations;           /* planes per rotation buffer (control.in's num_equations) */
 } pcl_device_view;
 typedef pcl_device_view pcl_bc_view;
 
@@ -333,13 +334,51 @@ int pcl_set_tile_rows(pcl_ctx* ctx, int rows);
      input's ghost cells, and is written only when *ierr = 1.
    - dt: the step size; ctl supplies the grid, limiter, boundary codes, grav, cfl_limit and
      dt_min_shrink_ratio (precision_mode must be FP64).  *cfl receives the attempt's CFL.
-   - stream: a cudaStream_t or NULL; the call synchronises it before returning.
+     Uniform grids and the built-in shallow-water module only: mapped meshes
+     (pcl_set_mesh_metrics) and other equation modules (pcl_set_equation) belong to contexts
+     and do not apply here.
+   - stream: a cudaStream_t or NULL; the call synchronises it before returning.  The caller's
+     current device is restored on return.
    The first call on a device looks up the array's device address (once per device); make that
-   first call before any stream capture.  All calls share the array and it keeps the last
-   call's contents; calls that overlap on the GPU race on it. */
+   first call before any stream capture.  The address belongs to the device's primary context:
+   after a cudaDeviceReset of that device, do not call this entry point on it again in the same
+   process.  All calls share the array and it keeps the last call's contents; calls that overlap
+   on the GPU race on it. */
 int pcl_solve_dimensional_split_noalloc(const pcl_solver_control* ctl, int device, void* stream,
                                         const double* d_state_in, double* d_state_out, long long ld,
                                         double dt, double* cfl, int* ierr);
+
+/* ---- self-checks of the FP64 sweeps' arithmetic shortcuts (no counterpart in the reference) ----
+   The FP64 sweeps take quotients that share a denominator from one correctly rounded reciprocal
+   (Markstein's correction, two steps), and skip the limiter's division where phi saturates; both
+   give the same bits as the plain IEEE operations.  These run the shortcut and the plain form side
+   by side on the current device and count results that differ in any bit. */
+/* a[k] / b[k] against the shared-reciprocal quotient for every pair inside the method's range
+   (|a|, |b|, |a/b| in [2^-960, 2^960], or a = 0); *checked = pairs in range. */
+int pcl_check_quotients(const double* a, const double* b, long long n, long long* mismatches, long long* checked);
+/* the same on n pseudo-random pairs generated on the device from seed */
+int pcl_check_quotients_random(long long n, unsigned long long seed, long long* mismatches, long long* checked);
+/* cell flux + HLL of both sweep directions, fast against plain division, on n random cell pairs
+   across the range the sweeps admit (h, |hu|, |hv| in [2^-64, 2^64), momenta also 0), with
+   gravity grav; the limiter with and without the saturation shortcut on waves made from them. */
+int pcl_check_flux_paths(long long n, unsigned long long seed, double grav, long long* flux_mismatches,
+                         long long* fast_pairs, long long* limiter_mismatches);
+
+/* ---- tests of the bounded-wait timeout path (no counterpart in the reference) ----
+   Every inter-CTA or copy-completion wait in the library is bounded; when one gives up, the
+   kernel records PCL_ERR_TIMEOUT, the attempt is void (the current solution stays as it was)
+   and the context or batch stays usable.  These switches make a wait run out on purpose, with
+   a short bound, so that path can be tested; both are off by default and set only from here.
+   Neither faults nor hangs the GPU: the wait is for a flag that nothing sets, and it ends at
+   its bound. */
+/* FP64 batch: the eta items of `slot` wait for one xi item more than the step has (slot -1:
+   off); spin_limit bounds every eta item's wait in polls of ~64 ns (0: the default, ~1 s).
+   pcl_batch_step then returns PCL_ERR_TIMEOUT and the slot's status is PCL_ERR_TIMEOUT. */
+int pcl_batch_inject_stall(pcl_batch* batch, int slot, unsigned spin_limit);
+/* Mixed-precision context: the bulk copy of state row `row` (-1 .. m_eta+2) into the fused
+   kernel's shared-memory ring is never issued, and its waits give up after `probes` probes
+   (row -1: off, the normal build runs again). */
+int pcl_inject_copy_stall(pcl_ctx* ctx, int row, unsigned probes);
 
 /* ---- utilities ---- */
 int pcl_synchronize(pcl_ctx* ctx);

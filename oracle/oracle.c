@@ -13,8 +13,10 @@
  * -march=native -O3, which lets gfortran contract; that build is not bit-reproducible).
  *
  * Array layout: the reference's column-major AoS vars(neq, -1:m_xi+2, -1:m_eta+2)
- * (domain/SMOD_domain_allocation.f90:94) with neq = 3 (h, hu, hv) fastest, then i, then j.
- * Work arrays keep the reference's shapes (solver/MOD_work_arrays.f90:61-69).
+ * (domain/SMOD_domain_allocation.f90:94) with neq = num_equations components fastest (the dam
+ * break: h, hu, hv), then i, then j.  Work arrays keep the reference's shapes
+ * (solver/MOD_work_arrays.f90:61-69) with num_waves = 2: HLL writes two waves, and the
+ * reference's further waves (num_waves > 2) stay zero after every flash_work_to_zero.
  *
  * Eigen modes for the HLL wave speed (solver/SMOD_approximate_Riemann_solvers.f90:63-72):
  *   0  closed form of the shallow-water Jacobian: eigenvalues u-c, u, u+c with
@@ -26,8 +28,6 @@
  *      faithful cost model of the reference and its closest runnable arithmetic.
  */
 #include "oracle.h"
-/* equation modules beyond the dam break (the caller's physics, shared with the CUDA path) */
-#include "../paraclaws_b200/csrc/pcl_equations.h"
 
 #include <dlfcn.h>
 #include <stdio.h>
@@ -40,7 +40,6 @@
 #endif
 
 #define UD_PRECISION 1e-10 /* constant/MOD_constants.f90:18 */
-#define NEQ 3
 #define NWAVES 2
 
 /* ------------------------------------------------------------------------------------- */
@@ -105,17 +104,18 @@ struct orc {
     tctl_t t;
     int status;
     double friction; /* source_function phi = (0, -c hu, -c hv); 0: phi = 0 */
-    int eq;          /* equation module (pcl_equations.h); 0: this file's shallow water */
+    int eq;          /* equation module (ORC_EQ_*) */
+    int neq;         /* num_equations: components per cell */
     double eqp[2];
 };
 
 #define CID(o, i, j) ((size_t)((j) + 1) * (size_t)(o)->ni + (size_t)((i) + 1))
-#define Q(o, me, i, j) (o)->vars[CID(o, i, j) * NEQ + (size_t)(me)]
+#define Q(o, me, i, j) (o)->vars[CID(o, i, j) * (size_t)(o)->neq + (size_t)(me)]
 #define LAM(o, mw, i, j) (o)->lambda[CID(o, i, j) * NWAVES + (size_t)(mw)]
-#define WAV(o, me, mw, i, j) (o)->waves[(CID(o, i, j) * NWAVES + (size_t)(mw)) * NEQ + (size_t)(me)]
-#define AM(o, me, i, j) (o)->Am[CID(o, i, j) * NEQ + (size_t)(me)]
-#define AP(o, me, i, j) (o)->Ap[CID(o, i, j) * NEQ + (size_t)(me)]
-#define FC(o, me, i, j) (o)->f[CID(o, i, j) * NEQ + (size_t)(me)]
+#define WAV(o, me, mw, i, j) (o)->waves[(CID(o, i, j) * NWAVES + (size_t)(mw)) * (size_t)(o)->neq + (size_t)(me)]
+#define AM(o, me, i, j) (o)->Am[CID(o, i, j) * (size_t)(o)->neq + (size_t)(me)]
+#define AP(o, me, i, j) (o)->Ap[CID(o, i, j) * (size_t)(o)->neq + (size_t)(me)]
+#define FC(o, me, i, j) (o)->f[CID(o, i, j) * (size_t)(o)->neq + (size_t)(me)]
 #define WNL(o, mw, i, j) (o)->wn2l[CID(o, i, j) * NWAVES + (size_t)(mw)]
 #define WNR(o, mw, i, j) (o)->wn2r[CID(o, i, j) * NWAVES + (size_t)(mw)]
 #define KAP(o, i, j) (o)->kappa[CID(o, i, j)]
@@ -302,112 +302,190 @@ static int jakobi(int ixy, const double* q, double g, double* J)
     return ORC_OK;
 }
 
-/* reference BLAS dgemv('N', 3, 3, 1.0, A, 3, x, 1, 0.0, y, 1) */
-static void matvec(int mode, const double* A, const double* x, double* y)
+/* ------------------------------------------------------------------------------------- */
+/* Other equation modules: the caller's physics through the getJakobi interface            */
+/* (user_subroutines/MOD_user_subroutines.f90), n = num_equations, J column-major n x n as   */
+/* Fortran jakobi(row, col) = J[(col-1)*n + (row-1)], with the eigenvalues                   */
+/* calculateEigenSolution would find (closed form in eigen mode 0, dgeev in mode 1).         */
+/* Restated here for the checker from each module's equations, independently of the         */
+/* library's own module code.                                                              */
+/* ------------------------------------------------------------------------------------- */
+int orc_module_num_equations(int eq)
+{
+    switch (eq) {
+    case ORC_EQ_OWN_SWE: case ORC_EQ_SWE: case ORC_EQ_ACOUSTICS: return 3;
+    case ORC_EQ_ADVECTION: case ORC_EQ_BURGERS: return 1;
+    case ORC_EQ_SWE_TRACER: return 4;
+    default: return 0;
+    }
+}
+
+/* the component a reflective wall negates on xi (ixy 1) / eta (ixy 2) sides; -1: mirror all */
+static int module_wall(int eq, int ixy)
+{
+    return (eq == ORC_EQ_ADVECTION || eq == ORC_EQ_BURGERS) ? -1 : ixy;
+}
+
+static int module_jakobi(int eq, const double* prm, int ixy, const double* q, double g, double* J)
+{
+    const int n = orc_module_num_equations(eq);
+    if (eq == ORC_EQ_OWN_SWE || eq == ORC_EQ_SWE) return jakobi(ixy, q, eq == ORC_EQ_SWE ? prm[0] : g, J);
+    for (int k = 0; k < n * n; ++k) J[k] = 0.0;
+#define JN(r, c) J[((c)-1) * n + ((r)-1)]
+    if (eq == ORC_EQ_ACOUSTICS) {
+        /* p_t + K (u_x + v_y) = 0, rho u_t + p_x = 0, rho v_t + p_y = 0 */
+        const double K = prm[0], rho = prm[1];
+        if (ixy == 1) {
+            JN(1, 2) = K;
+            JN(2, 1) = 1.0 / rho;
+        } else {
+            JN(1, 3) = K;
+            JN(3, 1) = 1.0 / rho;
+        }
+    } else if (eq == ORC_EQ_ADVECTION) {
+        /* q_t + a q_x + b q_y = 0 */
+        JN(1, 1) = ixy == 1 ? prm[0] : prm[1];
+    } else if (eq == ORC_EQ_BURGERS) {
+        /* Jacobian q in both directions */
+        JN(1, 1) = q[0];
+    } else if (eq == ORC_EQ_SWE_TRACER) {
+        /* the dam break's rows plus the transport of hc: flux (n hc)/h with n the normal momentum */
+        const double h = q[0], hu = q[1], hv = q[2], hc = q[3], gg = prm[0];
+        if (ixy == 1) {
+            JN(1, 1) = 0.0; JN(1, 2) = 1.0; JN(1, 3) = 0.0; JN(1, 4) = 0.0;
+            JN(2, 1) = -((hu * hu) / (h * h)) + gg * h; JN(2, 2) = (2.0 * hu) / h;
+            JN(3, 1) = -((hu * hv) / (h * h)); JN(3, 2) = hv / h; JN(3, 3) = hu / h;
+            JN(4, 1) = -((hu * hc) / (h * h)); JN(4, 2) = hc / h; JN(4, 4) = hu / h;
+        } else {
+            JN(1, 3) = 1.0;
+            JN(2, 1) = -((hu * hv) / (h * h)); JN(2, 2) = hv / h; JN(2, 3) = hu / h;
+            JN(3, 1) = -((hv * hv) / (h * h)) + gg * h; JN(3, 3) = (2.0 * hv) / h;
+            JN(4, 1) = -((hv * hc) / (h * h)); JN(4, 3) = hc / h; JN(4, 4) = hv / h;
+        }
+    }
+#undef JN
+    for (int k = 0; k < n * n; ++k)
+        if (isnan(J[k])) return ORC_ERR_NAN;
+    return ORC_OK;
+}
+
+/* closed-form eigenvalues of a module's Jacobian (real; the order does not matter to HLL) */
+static int module_eigen(int eq, const double* prm, int ixy, const double* q, double g, double* lam)
+{
+    if (eq == ORC_EQ_OWN_SWE || eq == ORC_EQ_SWE || eq == ORC_EQ_SWE_TRACER) {
+        const double gg = eq == ORC_EQ_OWN_SWE ? g : prm[0];
+        const double h = q[0];
+        if (h < 0.0) return ORC_ERR_NEG_DEPTH;
+        const double u = (ixy == 1 ? q[1] : q[2]) / h;
+        const double c = sqrt(gg * h);
+        lam[0] = u - c;
+        lam[1] = u;
+        lam[2] = u + c;
+        if (eq == ORC_EQ_SWE_TRACER) lam[3] = u;
+        return ORC_OK;
+    }
+    if (eq == ORC_EQ_ACOUSTICS) {
+        const double c = sqrt(prm[0] / prm[1]);
+        lam[0] = -c;
+        lam[1] = 0.0;
+        lam[2] = c;
+        return ORC_OK;
+    }
+    lam[0] = eq == ORC_EQ_BURGERS ? q[0] : (ixy == 1 ? prm[0] : prm[1]);
+    return ORC_OK;
+}
+
+/* reference BLAS dgemv('N', n, n, 1.0, A, n, x, 1, 0.0, y, 1) */
+static void matvec(int mode, int n, const double* A, const double* x, double* y)
 {
     if (mode == 1) {
-        const int n = 3, one = 1;
+        const int one = 1;
         const double alpha = 1.0, beta = 0.0;
         p_dgemv("N", &n, &n, &alpha, A, &n, x, &one, &beta, y, &one, 1);
         return;
     }
-    for (int r = 0; r < 3; ++r) y[r] = 0.0;
-    for (int c = 0; c < 3; ++c) {
+    for (int r = 0; r < n; ++r) y[r] = 0.0;
+    for (int c = 0; c < n; ++c) {
         const double temp = x[c];
-        for (int r = 0; r < 3; ++r) y[r] = y[r] + temp * A[c * 3 + r];
+        for (int r = 0; r < n; ++r) y[r] = y[r] + temp * A[c * n + r];
     }
 }
 
-/* calculateEigenSolution: real parts of the eigenvalues of J (utility/SMOD_eigenvalue_problem.f90) */
-static int eigenvalues(int mode, int ixy, const double* J, const double* q, double g, double* lam)
+/* calculateEigenSolution in eigen mode 1: LAPACK dgeev on the n x n Jacobian
+   (utility/SMOD_eigenvalue_problem.f90:33-88) */
+static int eigen_dgeev(int n, const double* J, double* lam)
 {
-    if (mode == 1) {
-        const int n = 3, one = 1;
-        double A[9], wr[3] = {0, 0, 0}, wi[3] = {0, 0, 0}, vl[1] = {0}, vr[9], wq[1] = {0};
-        int info = 0, lwork = -1;
-        memcpy(A, J, sizeof A);
-        memset(vr, 0, sizeof vr);
-        double* work = (double*)malloc(sizeof(double));
-        p_dgeev("N", "V", &n, A, &n, wr, wi, vl, &one, vr, &n, wq, &lwork, &info, 1, 1);
-        lwork = (int)wq[0];
-        free(work);
-        work = (double*)calloc((size_t)(lwork > 1 ? lwork : 1), sizeof(double));
-        p_dgeev("N", "V", &n, A, &n, wr, wi, vl, &one, vr, &n, work, &lwork, &info, 1, 1);
-        free(work);
-        for (int k = 0; k < 3; ++k) {
-            if (wi[k] > UD_PRECISION) return ORC_ERR_NEG_DEPTH; /* :72-83 */
-            lam[k] = wr[k];
-        }
-        return ORC_OK;
+    const int one = 1;
+    double A[ORC_MAX_EQ * ORC_MAX_EQ], wr[ORC_MAX_EQ], wi[ORC_MAX_EQ], vl[1] = {0},
+        vr[ORC_MAX_EQ * ORC_MAX_EQ], wq[1] = {0};
+    int info = 0, lwork = -1;
+    memcpy(A, J, sizeof(double) * (size_t)(n * n));
+    memset(vr, 0, sizeof vr);
+    memset(wr, 0, sizeof wr);
+    memset(wi, 0, sizeof wi);
+    double* work = (double*)malloc(sizeof(double));
+    p_dgeev("N", "V", &n, A, &n, wr, wi, vl, &one, vr, &n, wq, &lwork, &info, 1, 1);
+    lwork = (int)wq[0];
+    free(work);
+    work = (double*)calloc((size_t)(lwork > 1 ? lwork : 1), sizeof(double));
+    p_dgeev("N", "V", &n, A, &n, wr, wi, vl, &one, vr, &n, work, &lwork, &info, 1, 1);
+    free(work);
+    for (int k = 0; k < n; ++k) {
+        if (wi[k] > UD_PRECISION) return ORC_ERR_NEG_DEPTH; /* :72-83 */
+        lam[k] = wr[k];
     }
-    const double h = q[0];
-    if (h < 0.0) return ORC_ERR_NEG_DEPTH;
-    const double u = (ixy == 1 ? q[1] : q[2]) / h;
-    const double c = sqrt(g * h);
-    lam[0] = u - c;
-    lam[1] = u;
-    lam[2] = u + c;
     return ORC_OK;
 }
 
-/* HLL: solver/SMOD_approximate_Riemann_solvers.f90:15-102 for one interface */
-/* getJakobi / calculateEigenSolution of another equation module: its Jacobian, and in closed-form
-   mode its eigenvalues (mode 1 still calls dgeev on the module's Jacobian) */
-static int module_jakobi(int eq, const double* prm, int ixy, const double* q, double* J)
-{
-    return pcl_eq_jacobian(eq, ixy, q, prm, J) ? ORC_ERR_NAN : ORC_OK;
-}
-
+/* HLL: solver/SMOD_approximate_Riemann_solvers.f90:15-102 for one interface, n components */
 static int hll_core_eq(int eq, const double* prm, int ixy, const double* qL, const double* qR, double g, int mode,
-                       double* lam2, double* W);
-
-static int hll_core(int ixy, const double* qL, const double* qR, double g, int mode, double* lam2,
-                    double* W /* [mw*3+me] */)
+                       double* lam2, double* W /* [mw*n+me] */)
 {
-    return hll_core_eq(0, NULL, ixy, qL, qR, g, mode, lam2, W);
-}
-
-static int hll_core_eq(int eq, const double* prm, int ixy, const double* qL, const double* qR, double g, int mode,
-                       double* lam2, double* W /* [mw*3+me] */)
-{
-    double JL[9], JR[9], lL[3] = {0, 0, 0}, lR[3] = {0, 0, 0}, fL[3], fR[3];
+    const int n = orc_module_num_equations(eq);
+    double JL[ORC_MAX_EQ * ORC_MAX_EQ], JR[ORC_MAX_EQ * ORC_MAX_EQ], lL[ORC_MAX_EQ], lR[ORC_MAX_EQ],
+        fL[ORC_MAX_EQ], fR[ORC_MAX_EQ];
     int st = ORC_OK, s;
-    if ((s = eq ? module_jakobi(eq, prm, ixy, qL, JL) : jakobi(ixy, qL, g, JL)) != ORC_OK) st = s;
-    if ((s = eq ? module_jakobi(eq, prm, ixy, qR, JR) : jakobi(ixy, qR, g, JR)) != ORC_OK) st = s;
+    for (int k = 0; k < n; ++k) lL[k] = lR[k] = 0.0;
+    if ((s = module_jakobi(eq, prm, ixy, qL, g, JL)) != ORC_OK) st = s;
+    if ((s = module_jakobi(eq, prm, ixy, qR, g, JR)) != ORC_OK) st = s;
     if (st != ORC_OK) {
         lam2[0] = lam2[1] = 0.0;
-        for (int k = 0; k < 6; ++k) W[k] = 0.0;
+        for (int k = 0; k < 2 * n; ++k) W[k] = 0.0;
         return st;
     }
-    if (eq && mode == 0) {
-        if (pcl_eq_eigenvalues(eq, ixy, qL, prm, lL)) st = ORC_ERR_NEG_DEPTH;
-        if (pcl_eq_eigenvalues(eq, ixy, qR, prm, lR)) st = ORC_ERR_NEG_DEPTH;
+    if (mode == 1) {
+        if ((s = eigen_dgeev(n, JL, lL)) != ORC_OK) st = s;
+        if ((s = eigen_dgeev(n, JR, lR)) != ORC_OK) st = s;
     } else {
-        if ((s = eigenvalues(mode, ixy, JL, qL, g, lL)) != ORC_OK) st = s;
-        if ((s = eigenvalues(mode, ixy, JR, qR, g, lR)) != ORC_OK) st = s;
+        if ((s = module_eigen(eq, prm, ixy, qL, g, lL)) != ORC_OK) st = s;
+        if ((s = module_eigen(eq, prm, ixy, qR, g, lR)) != ORC_OK) st = s;
     }
-    /* s2 = maxval([abs(lambda_left), abs(lambda_right)]) :190 */
+    /* s2 = maxval([abs(lambda_left), abs(lambda_right)]) :66 */
     double s2 = fabs(lL[0]);
-    for (int k = 1; k < 3; ++k) s2 = fabs(lL[k]) > s2 ? fabs(lL[k]) : s2;
-    for (int k = 0; k < 3; ++k) s2 = fabs(lR[k]) > s2 ? fabs(lR[k]) : s2;
+    for (int k = 1; k < n; ++k) s2 = fabs(lL[k]) > s2 ? fabs(lL[k]) : s2;
+    for (int k = 0; k < n; ++k) s2 = fabs(lR[k]) > s2 ? fabs(lR[k]) : s2;
     double s1 = -s2;
     lam2[1] = s2;
     lam2[0] = s1;
-    fL[0] = fL[1] = fL[2] = 0.0;
-    fR[0] = fR[1] = fR[2] = 0.0;
+    for (int k = 0; k < n; ++k) fL[k] = fR[k] = 0.0;
     if (fabs(lam2[0]) > UD_PRECISION && fabs(lam2[1]) > UD_PRECISION) {
-        matvec(mode, JL, qL, fL);
-        matvec(mode, JR, qR, fR);
-        for (int me = 0; me < 3; ++me) {
+        matvec(mode, n, JL, qL, fL);
+        matvec(mode, n, JR, qR, fR);
+        for (int me = 0; me < n; ++me) {
             double qi = (((fR[me] - fL[me]) - s2 * qR[me]) + s1 * qL[me]) / ((UD_PRECISION + s1) - s2);
-            W[0 * 3 + me] = qi - qL[me];
-            W[1 * 3 + me] = qR[me] - qi;
+            W[0 * n + me] = qi - qL[me];
+            W[1 * n + me] = qR[me] - qi;
         }
     } else {
         lam2[0] = lam2[1] = 0.0;
-        for (int k = 0; k < 6; ++k) W[k] = 0.0;
+        for (int k = 0; k < 2 * n; ++k) W[k] = 0.0;
     }
     return st;
+}
+
+static int hll_core(int ixy, const double* qL, const double* qR, double g, int mode, double* lam2, double* W)
+{
+    return hll_core_eq(ORC_EQ_OWN_SWE, NULL, ixy, qL, qR, g, mode, lam2, W);
 }
 
 int orc_hll_interface(int ixy, const double* qL, const double* qR, double grav, int eigen_mode, double* lambda2,
@@ -419,9 +497,9 @@ int orc_hll_interface(int ixy, const double* qL, const double* qR, double grav, 
 
 static void wave_decomposition(orc_t* o, int ixy, int i, int j)
 {
-    double qL[3], qR[3], lam2[2], W[6];
+    double qL[ORC_MAX_EQ], qR[ORC_MAX_EQ], lam2[2], W[2 * ORC_MAX_EQ];
     const int il = ixy == 1 ? i - 1 : i, jl = ixy == 1 ? j : j - 1;
-    for (int me = 0; me < 3; ++me) {
+    for (int me = 0; me < o->neq; ++me) {
         qL[me] = Q(o, me, il, jl);
         qR[me] = Q(o, me, i, j);
     }
@@ -430,7 +508,7 @@ static void wave_decomposition(orc_t* o, int ixy, int i, int j)
     LAM(o, 0, i, j) = lam2[0];
     LAM(o, 1, i, j) = lam2[1];
     for (int mw = 0; mw < 2; ++mw)
-        for (int me = 0; me < 3; ++me) WAV(o, me, mw, i, j) = W[mw * 3 + me];
+        for (int me = 0; me < o->neq; ++me) WAV(o, me, mw, i, j) = W[mw * o->neq + me];
 }
 
 /* split_flux: solver/MOD_flux_calculation.f90:82-121 */
@@ -442,7 +520,7 @@ static void split_flux(orc_t* o)
         for (int i = 0; i <= mx + 1; ++i)
             for (int mw = 0; mw < 2; ++mw) {
                 const double s = LAM(o, mw, i, j);
-                for (int me = 0; me < 3; ++me) {
+                for (int me = 0; me < o->neq; ++me) {
                     const double w = WAV(o, me, mw, i, j);
                     const double mask = s < 0.0 ? 1.0 : 0.0;
                     AM(o, me, i, j) = AM(o, me, i, j) + mask * s * w;
@@ -468,7 +546,7 @@ static void integrate_flux_difference(orc_t* o, int ixy)
                 lrl = o->lr_eta[CID(o, i, j)];
                 lrr = o->lr_eta[CID(o, i, j + 1)];
             }
-            for (int me = 0; me < 3; ++me) {
+            for (int me = 0; me < o->neq; ++me) {
                 const double amr = ixy == 1 ? AM(o, me, i + 1, j) : AM(o, me, i, j + 1);
                 Q(o, me, i, j) = Q(o, me, i, j) - dtod / KAP(o, i, j) * (lrl * AP(o, me, i, j) + lrr * amr);
             }
@@ -495,13 +573,13 @@ static void limiter(orc_t* o, int ixy)
         const int i = 0;
         for (int j = 1; j <= my; ++j)
             for (int mw = 0; mw < 2; ++mw)
-                for (int me = 0; me < 3; ++me)
+                for (int me = 0; me < o->neq; ++me)
                     WNR(o, mw, i, j) = WNR(o, mw, i, j) + WAV(o, me, mw, i, j) * WAV(o, me, mw, i + 1, j);
     } else {
         const int j = 0;
         for (int i = 1; i <= mx; ++i)
             for (int mw = 0; mw < 2; ++mw)
-                for (int me = 0; me < 3; ++me)
+                for (int me = 0; me < o->neq; ++me)
                     WNR(o, mw, i, j) = WNR(o, mw, i, j) + WAV(o, me, mw, i, j) * WAV(o, me, mw, i, j + 1);
     }
     for (int j = 1; j <= my; ++j)
@@ -511,7 +589,7 @@ static void limiter(orc_t* o, int ixy)
                 WNL(o, mw, i, j) = ixy == 1 ? WNR(o, mw, i - 1, j) : WNR(o, mw, i, j - 1);
                 WNR(o, mw, i, j) = 0.0;
                 const int ir = i + (ixy == 1 ? 1 : 0), jr = j + (ixy == 1 ? 0 : 1);
-                for (int me = 0; me < 3; ++me) {
+                for (int me = 0; me < o->neq; ++me) {
                     wnorm2 = wnorm2 + WAV(o, me, mw, i, j) * WAV(o, me, mw, i, j);
                     WNR(o, mw, i, j) = WNR(o, mw, i, j) + WAV(o, me, mw, i, j) * WAV(o, me, mw, ir, jr);
                 }
@@ -519,7 +597,7 @@ static void limiter(orc_t* o, int ixy)
                 const double r = up / wnorm2;
                 const double phi = orc_limiter_phi(o->p.limiter_method, r);
                 if (!(fabs(wnorm2) <= UD_PRECISION))
-                    for (int me = 0; me < 3; ++me) WAV(o, me, mw, i, j) = phi * WAV(o, me, mw, i, j);
+                    for (int me = 0; me < o->neq; ++me) WAV(o, me, mw, i, j) = phi * WAV(o, me, mw, i, j);
             }
 }
 
@@ -537,7 +615,7 @@ static void second_order_flux_correction(orc_t* o, int ixy)
             const double kb = ixy == 1 ? 0.5 * (KAP(o, i - 1, j) + KAP(o, i, j)) : 0.5 * (KAP(o, i, j - 1) + KAP(o, i, j));
             for (int mw = 0; mw < 2; ++mw) {
                 const double al = fabs(LAM(o, mw, i, j));
-                for (int me = 0; me < 3; ++me)
+                for (int me = 0; me < o->neq; ++me)
                     FC(o, me, i, j) = FC(o, me, i, j) + 0.5 * al * (1.0 - al * dtod / kb) * WAV(o, me, mw, i, j);
             }
         }
@@ -552,7 +630,7 @@ static void integrator_flux_correction_increment(orc_t* o, int ixy)
 #pragma omp parallel for collapse(2)
     for (int j = 1; j <= my; ++j)
         for (int i = 1; i <= mx; ++i)
-            for (int me = 0; me < 3; ++me) {
+            for (int me = 0; me < o->neq; ++me) {
                 const double fr = ixy == 1 ? FC(o, me, i + 1, j) : FC(o, me, i, j + 1);
                 Q(o, me, i, j) = Q(o, me, i, j) - dtod / KAP(o, i, j) * (fr - FC(o, me, i, j));
             }
@@ -568,11 +646,11 @@ static void flash_work_to_zero(orc_t* o)
             o->wn2l[c * 2 + mw] = 0.0;
             o->wn2r[c * 2 + mw] = 0.0;
             o->lambda[c * 2 + mw] = 0.0;
-            for (int me = 0; me < 3; ++me) {
-                o->Am[c * 3 + me] = 0.0;
-                o->Ap[c * 3 + me] = 0.0;
-                o->waves[(c * 2 + mw) * 3 + me] = 0.0;
-                o->f[c * 3 + me] = 0.0;
+            for (int me = 0; me < o->neq; ++me) {
+                o->Am[c * o->neq + me] = 0.0;
+                o->Ap[c * o->neq + me] = 0.0;
+                o->waves[(c * 2 + mw) * o->neq + me] = 0.0;
+                o->f[c * o->neq + me] = 0.0;
             }
         }
     }
@@ -622,6 +700,7 @@ int orc_solve_dimensional_split(orc_t* o, int* ierr)
 {
     double cfl_local;
     *ierr = -1;
+    if (o->eq < 0) return ORC_ERR_BADARG; /* num_equations != 3 needs a module */
     cfl_local = sweep(o, 1);
     o->t.CFL = fmax(o->t.CFL, cfl_local); /* update_max_CFL */
     flash_work_to_zero(o);
@@ -651,52 +730,53 @@ int orc_update_rank_boundaries(orc_t* o)
     const int bcs[4] = {o->p.bc_xi_lower, o->p.bc_xi_upper, o->p.bc_eta_lower, o->p.bc_eta_upper};
     for (int k = 0; k < 4; ++k)
         if (bcs[k] < 1 || bcs[k] > 3) return ORC_ERR_BADARG;
+    const int wx = module_wall(o->eq, 1), wy = module_wall(o->eq, 2); /* wall: negated components */
     /* left */
     for (int j = 1; j <= my; ++j)
         for (int i = -1; i <= 0; ++i)
-            for (int me = 0; me < 3; ++me) {
+            for (int me = 0; me < o->neq; ++me) {
                 double v;
                 if (bcs[0] == 2) v = Q(o, me, 1, j);
                 else if (bcs[0] == 3)
                     v = Q(o, me, 1, j) + deriv_2p(o->xi[CID(o, 1, j)], o->xi[CID(o, 2, j)], Q(o, me, 1, j), Q(o, me, 2, j)) *
                                              (o->xi[CID(o, i, j)] - o->xi[CID(o, 1, j)]);
-                else v = me == 1 ? -Q(o, me, 1 - i, j) : Q(o, me, 1 - i, j);
+                else v = me == wx ? -Q(o, me, 1 - i, j) : Q(o, me, 1 - i, j);
                 Q(o, me, i, j) = v;
             }
     /* right */
     for (int j = 1; j <= my; ++j)
         for (int i = mx + 1; i <= mx + 2; ++i)
-            for (int me = 0; me < 3; ++me) {
+            for (int me = 0; me < o->neq; ++me) {
                 double v;
                 if (bcs[1] == 2) v = Q(o, me, mx, j);
                 else if (bcs[1] == 3)
                     v = Q(o, me, mx, j) + deriv_2p(o->xi[CID(o, mx - 1, j)], o->xi[CID(o, mx, j)], Q(o, me, mx - 1, j), Q(o, me, mx, j)) *
                                               (o->xi[CID(o, i, j)] - o->xi[CID(o, mx, j)]);
-                else v = me == 1 ? -Q(o, me, 2 * mx + 1 - i, j) : Q(o, me, 2 * mx + 1 - i, j);
+                else v = me == wx ? -Q(o, me, 2 * mx + 1 - i, j) : Q(o, me, 2 * mx + 1 - i, j);
                 Q(o, me, i, j) = v;
             }
     /* bottom */
     for (int j = -1; j <= 0; ++j)
         for (int i = 1; i <= mx; ++i)
-            for (int me = 0; me < 3; ++me) {
+            for (int me = 0; me < o->neq; ++me) {
                 double v;
                 if (bcs[2] == 2) v = Q(o, me, i, 1);
                 else if (bcs[2] == 3)
                     v = Q(o, me, i, 1) + deriv_2p(o->eta[CID(o, i, 1)], o->eta[CID(o, i, 2)], Q(o, me, i, 1), Q(o, me, i, 2)) *
                                              (o->eta[CID(o, i, j)] - o->eta[CID(o, i, 1)]);
-                else v = me == 2 ? -Q(o, me, i, 1 - j) : Q(o, me, i, 1 - j);
+                else v = me == wy ? -Q(o, me, i, 1 - j) : Q(o, me, i, 1 - j);
                 Q(o, me, i, j) = v;
             }
     /* top */
     for (int j = my + 1; j <= my + 2; ++j)
         for (int i = 1; i <= mx; ++i)
-            for (int me = 0; me < 3; ++me) {
+            for (int me = 0; me < o->neq; ++me) {
                 double v;
                 if (bcs[3] == 2) v = Q(o, me, i, my);
                 else if (bcs[3] == 3)
                     v = Q(o, me, i, my) + deriv_2p(o->eta[CID(o, i, my - 1)], o->eta[CID(o, i, my)], Q(o, me, i, my - 1), Q(o, me, i, my)) *
                                               (o->eta[CID(o, i, j)] - o->eta[CID(o, i, my)]);
-                else v = me == 2 ? -Q(o, me, i, 2 * my + 1 - j) : Q(o, me, i, 2 * my + 1 - j);
+                else v = me == wy ? -Q(o, me, i, 2 * my + 1 - j) : Q(o, me, i, 2 * my + 1 - j);
                 Q(o, me, i, j) = v;
             }
     return ORC_OK;
@@ -710,23 +790,27 @@ orc_t* orc_create(const orc_params* p)
     if (p->m_xi < 2 || p->m_eta < 2 || p->num_ghost != 2) return NULL;
     if (p->higher_order && p->use_limiter && (p->limiter_method < 1 || p->limiter_method > 4)) return NULL;
     if (p->eigen_mode == 1 && !p_dgeev) return NULL;
+    const int neq = p->num_equations == 0 ? 3 : p->num_equations;
+    if (neq < 1 || neq > ORC_MAX_EQ) return NULL;
     orc_t* o = (orc_t*)calloc(1, sizeof(orc_t));
     o->p = *p;
+    o->neq = neq;
+    o->eq = neq == 3 ? ORC_EQ_OWN_SWE : -1;
     o->ni = p->m_xi + 4;
     o->nj = p->m_eta + 4;
     const size_t nc = (size_t)o->ni * (size_t)o->nj;
-    o->vars = (double*)calloc(nc * NEQ, sizeof(double));
-    o->vars_old = (double*)calloc(nc * NEQ, sizeof(double));
+    o->vars = (double*)calloc(nc * (size_t)o->neq, sizeof(double));
+    o->vars_old = (double*)calloc(nc * (size_t)o->neq, sizeof(double));
     o->xi = (double*)calloc(nc, sizeof(double));
     o->eta = (double*)calloc(nc, sizeof(double));
     o->kappa = (double*)calloc(nc, sizeof(double));
     o->lr_xi = (double*)calloc(nc, sizeof(double));
     o->lr_eta = (double*)calloc(nc, sizeof(double));
     o->lambda = (double*)calloc(nc * NWAVES, sizeof(double));
-    o->waves = (double*)calloc(nc * NWAVES * NEQ, sizeof(double));
-    o->Am = (double*)calloc(nc * NEQ, sizeof(double));
-    o->Ap = (double*)calloc(nc * NEQ, sizeof(double));
-    o->f = (double*)calloc(nc * NEQ, sizeof(double));
+    o->waves = (double*)calloc(nc * NWAVES * (size_t)o->neq, sizeof(double));
+    o->Am = (double*)calloc(nc * (size_t)o->neq, sizeof(double));
+    o->Ap = (double*)calloc(nc * (size_t)o->neq, sizeof(double));
+    o->f = (double*)calloc(nc * (size_t)o->neq, sizeof(double));
     o->wn2l = (double*)calloc(nc * NWAVES, sizeof(double));
     o->wn2r = (double*)calloc(nc * NWAVES, sizeof(double));
     build_mesh(o);
@@ -751,11 +835,11 @@ int orc_status(const orc_t* o) { return o->status; }
 
 void orc_set_state(orc_t* o, const double* vars)
 {
-    memcpy(o->vars, vars, sizeof(double) * (size_t)o->ni * (size_t)o->nj * NEQ);
+    memcpy(o->vars, vars, sizeof(double) * (size_t)o->ni * (size_t)o->nj * (size_t)o->neq);
 }
 void orc_get_state(const orc_t* o, double* vars)
 {
-    memcpy(vars, o->vars, sizeof(double) * (size_t)o->ni * (size_t)o->nj * NEQ);
+    memcpy(vars, o->vars, sizeof(double) * (size_t)o->ni * (size_t)o->nj * (size_t)o->neq);
 }
 void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double* lr_xi, double* lr_eta)
 {
@@ -771,7 +855,7 @@ void orc_set_friction(orc_t* o, double c) { o->friction = c; }
 
 int orc_set_equation(orc_t* o, int module, double p0, double p1)
 {
-    if (module < 0 || module >= PCL_EQ_COUNT) return ORC_ERR_BADARG;
+    if (orc_module_num_equations(module) != o->neq) return ORC_ERR_BADARG;
     o->eq = module;
     o->eqp[0] = p0;
     o->eqp[1] = p1;
@@ -821,9 +905,10 @@ void orc_get_time_state(const orc_t* o, double* out8, int* out4)
 int orc_run(orc_t* o, long long max_attempts, double* log_d, int* log_i, long long log_cap, long long* n_attempts,
             long long* n_accepted)
 {
-    const size_t nbytes = sizeof(double) * (size_t)o->ni * (size_t)o->nj * NEQ;
+    const size_t nbytes = sizeof(double) * (size_t)o->ni * (size_t)o->nj * (size_t)o->neq;
     long long att = 0, acc = 0;
     int rc = ORC_OK;
+    if (o->eq < 0) return ORC_ERR_BADARG;
     while (o->t.time < o->t.time_final) {
         if (o->p.max_accepted > 0 && acc >= o->p.max_accepted) break;
         if (max_attempts > 0 && att >= max_attempts) break;
@@ -840,12 +925,12 @@ int orc_run(orc_t* o, long long max_attempts, double* log_d, int* log_i, long lo
         } else {
             /* integrate_source_term (MOD_solve.f90:295-336): with phi = 0 it is q + 0*dt, no change
                for finite q; with friction q_p = q_p + phi_p*dt per interior cell, j outer */
-            if (o->friction != 0.0) {
+            if (o->friction != 0.0 && o->neq == 3) {
                 const double dt = o->t.dt; /* get_dt(): updateTime has not run yet */
                 for (int j = 1; j <= o->p.m_eta; ++j)
                     for (int i = 1; i <= o->p.m_xi; ++i) {
                         const double phi[3] = {0.0, -o->friction * Q(o, 1, i, j), -o->friction * Q(o, 2, i, j)};
-                        for (int me = 0; me < NEQ; ++me) Q(o, me, i, j) = Q(o, me, i, j) + phi[me] * dt;
+                        for (int me = 0; me < 3; ++me) Q(o, me, i, j) = Q(o, me, i, j) + phi[me] * dt;
                     }
             }
             orc_update_rank_boundaries(o);

@@ -31,7 +31,7 @@ typedef struct orc_params {
     int n_snapshots;
     int adaptive;
     int eigen_mode;                      /* 0 closed form, 1 LAPACK dgeev + BLAS dgemv */
-    int pad0;
+    int num_equations;                   /* components per cell, 1 .. ORC_MAX_EQ (0: 3) */
     double xi_min, xi_max, eta_min, eta_max;
     double grav;
     double t_start, t_final, dt_initial;
@@ -57,7 +57,7 @@ int    orc_status(const orc_t* o);
 void   orc_set_threads(int n);
 int    orc_get_threads(void);
 
-/* state in the reference layout vars(3, -1:m_xi+2, -1:m_eta+2), column-major */
+/* state in the reference layout vars(num_equations, -1:m_xi+2, -1:m_eta+2), column-major */
 void orc_set_state(orc_t* o, const double* vars);
 void orc_get_state(const orc_t* o, double* vars);
 
@@ -67,8 +67,20 @@ void orc_get_mesh(const orc_t* o, double* xi, double* eta, double* kappa, double
    friction), integrated by integrate_source_term (solver/MOD_solve.f90:295-336); c = 0 is the
    dam break's phi = 0 */
 void orc_set_friction(orc_t* o, double c);
-/* equation module of paraclaws_b200/csrc/pcl_equations.h (0: this oracle's own shallow-water
-   restatement); shallow water takes p0 = g, acoustics p0 = K, p1 = rho */
+/* Equation modules (getJakobi of user_subroutines/MOD_user_subroutines.f90 and the eigenvalues
+   of its Jacobian), restated in oracle.c for the checker.  The ids are the ones the library's
+   pcl_set_equation takes, so a test passes the same id to both; num_equations of the module
+   must be the context's. */
+enum {
+    ORC_EQ_OWN_SWE = 0,    /* the dam-break shallow water, g from orc_params (3 equations) */
+    ORC_EQ_SWE = 1,        /* the same Jacobian with g = p0 (3) */
+    ORC_EQ_ACOUSTICS = 2,  /* linear acoustics (p, u, v), p0 = K, p1 = rho (3) */
+    ORC_EQ_ADVECTION = 3,  /* q_t + a q_x + b q_y = 0, p0 = a, p1 = b (1) */
+    ORC_EQ_BURGERS = 4,    /* Jacobian q in both directions (1) */
+    ORC_EQ_SWE_TRACER = 5  /* (h, hu, hv, hc): shallow water carrying a tracer, p0 = g (4) */
+};
+#define ORC_MAX_EQ 4
+int orc_module_num_equations(int module);
 int orc_set_equation(orc_t* o, int module, double p0, double p1);
 /* replace capacity and face length ratios by those of a mapped grid (finalize_mesh of a user
    mapping, SMOD_mesh_manipulation.f90:147-173); cell centres stay computational */

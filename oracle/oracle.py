@@ -31,7 +31,7 @@ class OrcParams(C.Structure):
         ("m_xi", C.c_int), ("m_eta", C.c_int), ("num_ghost", C.c_int), ("higher_order", C.c_int),
         ("use_limiter", C.c_int), ("limiter_method", C.c_int), ("bc_xi_lower", C.c_int),
         ("bc_xi_upper", C.c_int), ("bc_eta_lower", C.c_int), ("bc_eta_upper", C.c_int),
-        ("n_snapshots", C.c_int), ("adaptive", C.c_int), ("eigen_mode", C.c_int), ("pad0", C.c_int),
+        ("n_snapshots", C.c_int), ("adaptive", C.c_int), ("eigen_mode", C.c_int), ("num_equations", C.c_int),
         ("xi_min", C.c_double), ("xi_max", C.c_double), ("eta_min", C.c_double), ("eta_max", C.c_double),
         ("grav", C.c_double), ("t_start", C.c_double), ("t_final", C.c_double), ("dt_initial", C.c_double),
         ("cfl_limit", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double), ("growth", C.c_double),
@@ -69,6 +69,7 @@ def lib():
         L.orc_set_mesh.argtypes = [C.c_void_p, dp, dp, dp]
         L.orc_set_friction.argtypes = [C.c_void_p, C.c_double]
         L.orc_set_equation.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+        L.orc_module_num_equations.argtypes = [C.c_int]
         L.orc_update_rank_boundaries.argtypes = [C.c_void_p]
         L.orc_solve_dimensional_split.argtypes = [C.c_void_p, P(C.c_int)]
         L.orc_sweep.argtypes = [C.c_void_p, C.c_int, P(C.c_double)]
@@ -120,6 +121,7 @@ def params_from(control, custom=None, eigen_mode: int = 0) -> OrcParams:
     p.n_snapshots = control.number_of_snapshots
     p.adaptive = int(bool(control.adaptive_timestepping))
     p.eigen_mode = eigen_mode
+    p.num_equations = int(control.number_of_equations)
     p.xi_min, p.xi_max = float(control.xi_min), float(control.xi_max)
     p.eta_min, p.eta_max = float(control.eta_min), float(control.eta_max)
     p.grav = float(custom.grav) if custom is not None else GRAV_REFERENCE
@@ -155,7 +157,7 @@ class Oracle:
         self.h = L.orc_create(C.byref(self.p))
         if not self.h:
             raise ValueError("oracle rejected the settings")
-        self.shape = (control.m_eta + 4, control.m_xi + 4, 3)
+        self.shape = (control.m_eta + 4, control.m_xi + 4, int(control.number_of_equations))
 
     def close(self):
         if self.h:
@@ -185,8 +187,10 @@ class Oracle:
         lib().orc_set_friction(self.h, float(c))
 
     def set_equation(self, module: int, p0: float = 0.0, p1: float = 0.0) -> None:
+        """Equation module (ORC_EQ_* of oracle.h: the same ids as the library's PCL_EQ_*), whose
+        num_equations must be the context's."""
         if lib().orc_set_equation(self.h, int(module), float(p0), float(p1)) != 0:
-            raise ValueError(f"unknown equation module {module}")
+            raise ValueError(f"equation module {module} does not fit this context")
 
     def set_mesh(self, kappa, lr_xi, lr_eta) -> None:
         """Metrics of a mapped grid (arrays shaped like mesh()['kappa'])."""

@@ -146,6 +146,12 @@ def load(build_if_missing: bool = True):
     L.pcl_set_tile_rows.argtypes = [vp, C.c_int]
     L.pcl_solve_dimensional_split_noalloc.argtypes = [P(SolverControl), C.c_int, vp, vp, vp, C.c_longlong,
                                                       C.c_double, P(C.c_double), P(C.c_int)]
+    L.pcl_check_quotients.argtypes = [vp, vp, C.c_longlong, P(C.c_longlong), P(C.c_longlong)]
+    L.pcl_check_quotients_random.argtypes = [C.c_longlong, C.c_ulonglong, P(C.c_longlong), P(C.c_longlong)]
+    L.pcl_check_flux_paths.argtypes = [C.c_longlong, C.c_ulonglong, C.c_double, P(C.c_longlong),
+                                       P(C.c_longlong), P(C.c_longlong)]
+    L.pcl_batch_inject_stall.argtypes = [vp, C.c_int, C.c_uint]
+    L.pcl_inject_copy_stall.argtypes = [vp, C.c_int, C.c_uint]
     L.pcl_host_alloc.argtypes = [P(vp), C.c_longlong]
     L.pcl_host_free.argtypes = [vp]
     L.pcl_status_string.argtypes = [C.c_int]

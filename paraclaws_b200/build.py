@@ -23,6 +23,7 @@ HEADERS = [ROOT / "include" / "paraclaws_b200.h"] + sorted(CSRC.glob("*.h")) + s
 # (source, allow FMA contraction)
 SOURCES = [
     ("kernels_fp64.cu", False),
+    ("kernels_gen.cu", False),
     ("kernels_aux.cu", False),
     ("kernels_mixed.cu", False),
     ("batch_fp64.cu", False),
@@ -30,6 +31,7 @@ SOURCES = [
     ("capi.cu", False),
     ("capi_batch.cu", False),
     ("noalloc.cu", False),
+    ("selfcheck.cu", False),
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -91,6 +91,11 @@ IC_CIRCULAR_DAM = 1  # examples/2D_dam_break/cartesian/SMOD_set_initial_conditio
 EQ_SHALLOW_WATER = 0
 EQ_SHALLOW_WATER_GENERIC = 1
 EQ_ACOUSTICS = 2
+EQ_ADVECTION = 3              # one equation, params (a, b)
+EQ_BURGERS = 4                # one equation, no params
+EQ_SHALLOW_WATER_TRACER = 5   # four equations (h, hu, hv, hc), params (g)
+EQ_NUM_EQUATIONS = {EQ_SHALLOW_WATER: 3, EQ_SHALLOW_WATER_GENERIC: 3, EQ_ACOUSTICS: 3, EQ_ADVECTION: 1,
+                    EQ_BURGERS: 1, EQ_SHALLOW_WATER_TRACER: 4}
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -196,9 +201,11 @@ def read_custom(path: Path | str) -> CustomSettings:
 
 
 def validate(control: ControlSettings) -> None:
-    """Reject settings outside what the shallow-water hot path supports."""
-    if control.number_of_equations != 3 or control.number_of_waves != 2:
-        raise ValueError("the shallow-water equation module has 3 equations and 2 waves")
+    """Reject settings outside what the step supports: 1 .. 4 equations (the equation modules'
+    sizes; 3 for the shallow-water modules), at least the two waves HLL makes (further waves stay
+    zero in the reference and change nothing)."""
+    if not 1 <= control.number_of_equations <= 4 or control.number_of_waves < 2:
+        raise ValueError("num_equations must be 1 .. 4 and num_waves at least 2 (HLL makes two waves)")
     if control.number_of_ghost_cells != 2:
         raise ValueError("the second-order correction needs exactly 2 ghost layers")
     if control.m_xi < 2 or control.m_eta < 2:

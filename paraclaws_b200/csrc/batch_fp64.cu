@@ -27,10 +27,13 @@ __device__ __forceinline__ void run_item(const GridDev& g, int kind, int a, int 
                                          XSmem<kThreads>& S) {
   if (kind == kItemX) {
     const int jend = min(a + v.x_rows - 1, g.my);
+    double smax = 0.0;
+    int bad = 0;
     for (int j = a; j <= jend; ++j) {
-      xsweep_segment<kThreads, LIM, SO, MK>(g, j, b, S);
+      xsweep_segment<kThreads, LIM, SO, MK>(g, j, b, S, smax, bad);
       __syncthreads();  // the segment's shared arrays are reused by the next row
     }
+    xsweep_finish<kThreads>(g, smax, bad, S);
   } else {
     ysweep_strip<LIM, SO, MK>(g, a, b, v.y_rows);
   }
@@ -81,14 +84,17 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
       if (w.y == kItemY) {
         // wait for every xi item of this instance (bounded; they are all in flight or done)
         if (threadIdx.x == 0) {
-          const int need = v.totals[2 * w.x];
+          const int need = v.totals[2 * w.x] + (w.x == v.stall_slot ? 1 : 0);
           unsigned k = 0;
           while (atomicAdd(xdone, 0) < need && k < v.spin_limit) {
             __nanosleep(64);
             ++k;
           }
           s_flag = atomicAdd(xdone, 0) >= need;
-          if (!s_flag) atomicOr(&ctl->status, kStatusTimeout);
+          if (!s_flag) {
+            atomicOr(&ctl->status, kStatusTimeout);
+            atomicOr(v.flags, 1);
+          }
           __threadfence();
         }
         __syncthreads();

@@ -25,26 +25,27 @@ namespace {
 using mixed::NT;
 using mixed::Smem;
 
+// Each returns false when a bounded wait of the item gave up (mixed_item).
 template <class G>
-__device__ __forceinline__ void dispatch_item(const G& g, int mode, int strip, int seg, int ty, Smem& S,
+__device__ __forceinline__ bool dispatch_item(const G& g, int mode, int strip, int seg, int ty, Smem& S,
                                               unsigned& rows) {
   switch (mode) {
-    case 0: mixed::mixed_item<0, false>(g, strip, seg, ty, S, rows); break;
-    case 2: mixed::mixed_item<1, true>(g, strip, seg, ty, S, rows); break;
-    case 3: mixed::mixed_item<2, true>(g, strip, seg, ty, S, rows); break;
-    case 4: mixed::mixed_item<3, true>(g, strip, seg, ty, S, rows); break;
-    case 5: mixed::mixed_item<4, true>(g, strip, seg, ty, S, rows); break;
-    default: mixed::mixed_item<0, true>(g, strip, seg, ty, S, rows); break;
+    case 0: return mixed::mixed_item<0, false>(g, strip, seg, ty, S, rows);
+    case 2: return mixed::mixed_item<1, true>(g, strip, seg, ty, S, rows);
+    case 3: return mixed::mixed_item<2, true>(g, strip, seg, ty, S, rows);
+    case 4: return mixed::mixed_item<3, true>(g, strip, seg, ty, S, rows);
+    case 5: return mixed::mixed_item<4, true>(g, strip, seg, ty, S, rows);
+    default: return mixed::mixed_item<0, true>(g, strip, seg, ty, S, rows);
   }
 }
 
 // One mode only: the row loop unrolled by two, as in the single-grid kernel (it still fits five
 // CTAs per SM when the kernel holds one item body instead of six).
 template <int MODE, class G>
-__device__ __forceinline__ void mode_item(const G& g, int strip, int seg, int ty, Smem& S, unsigned& rows) {
-  if (MODE == 0) mixed::mixed_item<0, false, 2>(g, strip, seg, ty, S, rows);
-  else if (MODE == 1) mixed::mixed_item<0, true, 2>(g, strip, seg, ty, S, rows);
-  else mixed::mixed_item<(MODE >= 2 ? MODE - 1 : 0), true, 2>(g, strip, seg, ty, S, rows);
+__device__ __forceinline__ bool mode_item(const G& g, int strip, int seg, int ty, Smem& S, unsigned& rows) {
+  if (MODE == 0) return mixed::mixed_item<0, false, 2>(g, strip, seg, ty, S, rows);
+  if (MODE == 1) return mixed::mixed_item<0, true, 2>(g, strip, seg, ty, S, rows);
+  return mixed::mixed_item<(MODE >= 2 ? MODE - 1 : 0), true, 2>(g, strip, seg, ty, S, rows);
 }
 
 __device__ __forceinline__ int item_mode(const GridDev& g) { return g.second_order ? 1 + g.limiter : 0; }
@@ -93,25 +94,27 @@ __global__ void __launch_bounds__(NT, POOL ? 5 : 4) batch_mixed_kernel(BatchView
     if (it >= n) break;
     const int4 w = v.items[it];
     Ctl* ctl;
+    bool ok = true;
     if (POOL) {
       const ItemDesc& d = c_desc[v.desc_base + w.x];
       ctl = d.ctl;
       if (!ctl->done) {
         if (MODE >= 0)
-          mode_item<MODE>(d, w.z, w.w, v.tile_rows, S, rows);
+          ok = mode_item<MODE>(d, w.z, w.w, v.tile_rows, S, rows);
         else
-          dispatch_item(d, d.mode, w.z, w.w, v.tile_rows, S, rows);
-        if (IG && edge_item(d.mx, d.my, w.z, w.w, v.tile_rows))
+          ok = dispatch_item(d, d.mode, w.z, w.w, v.tile_rows, S, rows);
+        if (ok && IG && edge_item(d.mx, d.my, w.z, w.w, v.tile_rows))
           item_ghosts(v.inst[w.x], w.z, w.w, v.tile_rows);
       }
     } else {
       const GridDev g = v.inst[w.x];
       ctl = g.ctl;
       if (!ctl->done) {
-        dispatch_item(g, item_mode(g), w.z, w.w, v.tile_rows, S, rows);
-        if (IG && edge_item(g.mx, g.my, w.z, w.w, v.tile_rows)) item_ghosts(g, w.z, w.w, v.tile_rows);
+        ok = dispatch_item(g, item_mode(g), w.z, w.w, v.tile_rows, S, rows);
+        if (ok && IG && edge_item(g.mx, g.my, w.z, w.w, v.tile_rows)) item_ghosts(g, w.z, w.w, v.tile_rows);
       }
     }
+    if (!ok && threadIdx.x == 0) atomicOr(v.flags, 1);
     int* alldone = v.counters + 2 * w.x + 1;
     __threadfence();  // every thread's writes of this item precede its completion count
     __syncthreads();
@@ -136,6 +139,10 @@ __global__ void __launch_bounds__(NT, POOL ? 5 : 4) batch_mixed_kernel(BatchView
       }
     }
     __syncthreads();
+    // After a wait gave up, this CTA's row ring is out of phase: it takes no further items (the
+    // queue hands them to the other CTAs; the item was counted, so its instance still finishes
+    // the step, as a void attempt).
+    if (!ok) break;
   }
 }
 

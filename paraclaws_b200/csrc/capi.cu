@@ -228,8 +228,17 @@ int pcl_read_solver_control(const char* control_in, const char* custom_in, pcl_s
   return PCL_OK;
 }
 
+// num_equations: the state's components, 1 .. PCL_EQ_MAX_EQUATIONS (3 for the shallow-water
+// modules, the mixed-precision and batched forms).  num_waves: HLL makes two waves
+// (solver/SMOD_approximate_Riemann_solvers.f90:68-100 writes lambda(1:2) and waves(:,1:2)); the
+// reference's work arrays hold num_waves of them, zeroed after every sweep
+// (solver/MOD_work_arrays.f90:79-109), so waves 3.. stay zero and add nothing to the CFL maximum,
+// the split fluxes or the correction: any num_waves >= 2 runs the two-wave step.  num_waves = 1
+// would have HLL write past its arrays and is refused.
 int validate_control(const pcl_solver_control* c) {
-  if (c->num_equations != 3 || c->num_waves != 2 || c->num_ghost != 2) return PCL_ERR_BADARG;
+  if (c->num_equations < 1 || c->num_equations > PCL_EQ_MAX_EQUATIONS || c->num_waves < 2 || c->num_ghost != 2)
+    return PCL_ERR_BADARG;
+  if (c->num_equations != 3 && c->precision_mode != PCL_PREC_FP64) return PCL_ERR_BADARG;
   if (c->m_xi < 2 || c->m_eta < 2) return PCL_ERR_BADARG;
   if (c->m_xi > (1 << 28) || c->m_eta > 16 * 65535) return PCL_ERR_BADARG;  // launch-grid limits
   const int bcs[4] = {c->bc_xi_lower, c->bc_xi_upper, c->bc_eta_lower, c->bc_eta_upper};
@@ -332,13 +341,14 @@ int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
   const int ni = c->m_xi + 4, nj = c->m_eta + 4;
   const int pitch = (ni + 31) / 32 * 32;
   const long long plane = (long long)pitch * nj;
-  const size_t buf_bytes = sizeof(double) * 3 * 3 * (size_t)plane;
+  const int neq = c->num_equations;
+  const size_t buf_bytes = sizeof(double) * 3 * (size_t)neq * (size_t)plane;
   const double dxi = (c->xi_max - c->xi_min) / c->m_xi;     // :28
   const double deta = (c->eta_max - c->eta_min) / c->m_eta;  // :29
   std::vector<double> rowm, colm;
   build_tables(c, dxi, deta, rowm, colm);
   const size_t tab_bytes = sizeof(double) * (rowm.size() + colm.size());
-  const size_t stg_bytes = sizeof(double) * 3 * (size_t)ni * nj;
+  const size_t stg_bytes = sizeof(double) * (size_t)neq * (size_t)ni * nj;
   x->log_cap = 1 << 16;
   if (cudaMalloc(&x->bufs_d, buf_bytes) != cudaSuccess) return fail(PCL_ERR_OOM);
   if (cudaMalloc(&x->tables_d, tab_bytes) != cudaSuccess) return fail(PCL_ERR_OOM);
@@ -360,7 +370,9 @@ int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
     return fail(PCL_ERR_CUDA);
   GridDev& g = x->g;
   g.state = x->bufs_d;
-  g.bufstride = 3 * plane;
+  g.bufstride = (long long)neq * plane;
+  g.neq = neq;
+  g.eq = neq == 3 ? PCL_EQ_SHALLOW_WATER : -1;  // other sizes need a module (pcl_set_equation)
   g.rowm = x->tables_d;
   g.colm = x->tables_d + rowm.size();
   g.ctl = x->ctl_d;
@@ -399,7 +411,9 @@ int pcl_destroy(pcl_ctx* x) {
   return PCL_OK;
 }
 
-long long pcl_state_doubles(const pcl_ctx* x) { return x ? 3LL * (x->cfg.m_xi + 4) * (x->cfg.m_eta + 4) : 0; }
+long long pcl_state_doubles(const pcl_ctx* x) {
+  return x ? (long long)x->cfg.num_equations * (x->cfg.m_xi + 4) * (x->cfg.m_eta + 4) : 0;
+}
 long long pcl_device_bytes(const pcl_ctx* x) { return x ? (long long)x->device_bytes : 0; }
 void* pcl_get_stream(pcl_ctx* x) { return x ? (void*)x->stream : nullptr; }
 
@@ -441,7 +455,7 @@ int pcl_upload_state(pcl_ctx* x, const double* vars) {
 
 int pcl_initial_condition(pcl_ctx* x) {
   if (!x) return PCL_ERR_BADARG;
-  if (x->cfg.initial_condition != 1) return PCL_ERR_BADARG;
+  if (x->cfg.initial_condition != 1 || x->g.neq != 3) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   const pcl_solver_control& c = x->cfg;
   launch_dam_ic(x->g, c.dam_radius, c.dam_h_in, c.dam_h_out, c.dam_x0, c.dam_y0, x->stream);
@@ -477,6 +491,7 @@ static void fill_view(const pcl_ctx* x, pcl_device_view& v) {
   v.current_buffer = &x->ctl_d->cur;
   v.attempt_accepted = &x->ctl_d->ierr;
   v.step_dt = &x->ctl_d->dt_step;
+  v.num_equations = x->g.neq;
 }
 
 // The ghost fill: the built-in kernel for every side, then the user hook for sides coded 1.
@@ -554,7 +569,7 @@ static void launch_sweeps(pcl_ctx* x) {
 }
 
 int pcl_solve_dimensional_split(pcl_ctx* x, int* ierr) {
-  if (!x || !ierr) return PCL_ERR_BADARG;
+  if (!x || !ierr || x->g.eq < 0) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   launch_sweeps(x);
   launch_timectl(x->g, kOpFinalizeSolve, 0, 0.0, x->stream);
@@ -699,7 +714,7 @@ int pcl_advance_to_snapshot(pcl_ctx* x, pcl_run_stats* stats) {
 }
 
 static int advance_loop(pcl_ctx* x, long long max_attempts, pcl_run_stats* stats) {
-  if (!x) return PCL_ERR_BADARG;
+  if (!x || x->g.eq < 0) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   const int chunk = 32;
   int r = build_graph(x, chunk);
@@ -749,7 +764,7 @@ int pcl_reset_time_control(pcl_ctx* x) {
 }
 
 int pcl_profile_kernels(pcl_ctx* x, int reps, double* avg_ms, int* nkinds) {
-  if (!x || !avg_ms || reps < 1) return PCL_ERR_BADARG;
+  if (!x || !avg_ms || reps < 1 || x->g.eq < 0) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   const int nk = sweep_kernels(x) + 2;
   cudaEvent_t ev[6];
@@ -809,7 +824,7 @@ int pcl_get_step_log(pcl_ctx* x, pcl_step_record* out, long long cap, long long*
 }
 
 int pcl_conservation_sums(pcl_ctx* x, double* sums) {
-  if (!x || !sums) return PCL_ERR_BADARG;
+  if (!x || !sums || x->g.neq != 3) return PCL_ERR_BADARG;
   CK(cudaSetDevice(x->device));
   // the AoS staging buffer (3 doubles per padded cell) holds the 3 partials of each row
   launch_row_sums(x->g, x->staging_d, x->stream);
@@ -837,6 +852,8 @@ static void drop_graph(pcl_ctx* x) {
 
 int pcl_set_equation(pcl_ctx* x, int module, const double* params, int nparams) {
   if (!x || module < 0 || module >= PCL_EQ_COUNT || nparams < 0 || (nparams > 0 && !params)) return PCL_ERR_BADARG;
+  // the module's num_equations is the context's (control.in): the state has that many planes
+  if (pcl_eq_num_equations(module) != x->cfg.num_equations) return PCL_ERR_BADARG;
   if (module != PCL_EQ_SHALLOW_WATER && (x->cfg.precision_mode != PCL_PREC_FP64 || x->g.metric == kMetricMapped))
     return PCL_ERR_BADARG;
   double p[2] = {x->cfg.grav, 0.0};
@@ -844,7 +861,13 @@ int pcl_set_equation(pcl_ctx* x, int module, const double* params, int nparams) 
     if (nparams != 2 || !(params[0] > 0.0) || !(params[1] > 0.0)) return PCL_ERR_BADARG;
     p[0] = params[0];
     p[1] = params[1];
-  } else if (nparams >= 1) {
+  } else if (module == PCL_EQ_ADVECTION) {
+    if (nparams != 2 || !std::isfinite(params[0]) || !std::isfinite(params[1])) return PCL_ERR_BADARG;
+    p[0] = params[0];
+    p[1] = params[1];
+  } else if (module == PCL_EQ_BURGERS) {
+    if (nparams != 0) return PCL_ERR_BADARG;
+  } else if (nparams >= 1) {  // the shallow-water modules: g
     p[0] = params[0];
   }
   x->g.eq = module;
@@ -927,6 +950,13 @@ int pcl_set_tile_rows(pcl_ctx* x, int rows) {
   if (!x || rows < 4) return PCL_ERR_BADARG;
   if (x->mixed) mixed_set_tile_rows(x->mixed, rows);
   drop_graph(x);  // the captured launches carry the old tiling
+  return PCL_OK;
+}
+
+int pcl_inject_copy_stall(pcl_ctx* x, int row, unsigned probes) {
+  if (!x || !x->mixed || row < -1 || row > x->cfg.m_eta + 2) return PCL_ERR_BADARG;
+  mixed_set_injection(x->mixed, row, probes);
+  drop_graph(x);  // the captured launches run the other build
   return PCL_OK;
 }
 
@@ -1043,12 +1073,13 @@ int pcl_write_snapshot(pcl_ctx* x, const char* output_dir, int wait) {
   const std::string sub = dir + "/rank_0";
   const long long cells = (long long)(x->cfg.m_xi + 4) * (x->cfg.m_eta + 4);
   const int naux = x->cfg.num_aux;
+  const int neq = x->cfg.num_equations;
   x->snap_status = PCL_OK;
-  x->snap_thread = std::thread([x, dir, sub, cells, naux] {
+  x->snap_thread = std::thread([x, dir, sub, cells, naux, neq] {
     int st = PCL_OK;
     if (cudaEventSynchronize(x->snap_ev) != cudaSuccess) st = PCL_ERR_CUDA;
     if (st == PCL_OK && !(make_dir(dir) && make_dir(sub))) st = PCL_ERR_IO;
-    if (st == PCL_OK && !write_records(sub + "/qout.dat", x->snap_h, cells, 3)) st = PCL_ERR_IO;
+    if (st == PCL_OK && !write_records(sub + "/qout.dat", x->snap_h, cells, neq)) st = PCL_ERR_IO;
     // the SWE never sets its aux fields: num_aux zeros per cell
     if (st == PCL_OK && !write_records(sub + "/aout.dat", nullptr, cells, naux)) st = PCL_ERR_IO;
     x->snap_status = st;

@@ -67,7 +67,8 @@ struct pcl_batch {
   GridDev* inst_d = nullptr;
   int4* items_d = nullptr;
   long long items_cap = 0;
-  int* scal_d = nullptr;       // [0] n_items, [1] queue head
+  int* scal_d = nullptr;       // [0] n_items, [1] queue head, [2] timeout flags of the last steps
+  int* flags_h = nullptr;      // pinned copy of scal_d[2]
   int* counters_d = nullptr;
   int* totals_d = nullptr;
   int* poll_d = nullptr;       // [4*max_slots]: used flags, then done/status/accepted per slot
@@ -87,6 +88,8 @@ struct pcl_batch {
   int graph_chunk = 0;
   long long launches = 0;
   long long steps = 0;
+  unsigned spin_limit = 1u << 24;  // bounded wait of an FP64 eta item (about a second)
+  int stall_slot = -1;             // pcl_batch_inject_stall
 };
 
 #define BCK(call)                                                                          \
@@ -125,7 +128,9 @@ static BatchView view(const pcl_batch* b) {
   v.tile_rows = b->tile_rows_eff;
   v.desc_base = b->desc_base;
   v.item_ghosts = b->item_ghosts;
-  v.spin_limit = 1u << 24;
+  v.spin_limit = b->spin_limit;
+  v.flags = b->scal_d + 2;
+  v.stall_slot = b->stall_slot;
   return v;
 }
 
@@ -287,6 +292,7 @@ int pcl_batch_create(int device, int precision, int max_instances, pcl_batch** o
     cudaFree(b->totals_d);
     cudaFree(b->poll_d);
     if (b->ctl_h) cudaFreeHost(b->ctl_h);
+    if (b->flags_h) cudaFreeHost(b->flags_h);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return code;
@@ -298,6 +304,8 @@ int pcl_batch_create(int device, int precision, int max_instances, pcl_batch** o
   if (cudaMalloc(&b->totals_d, sizeof(int) * 2 * max_instances) != cudaSuccess) return fail(PCL_ERR_OOM);
   if (cudaMalloc(&b->poll_d, sizeof(int) * 4 * max_instances) != cudaSuccess) return fail(PCL_ERR_OOM);
   if (cudaMallocHost(&b->ctl_h, sizeof(Ctl)) != cudaSuccess) return fail(PCL_ERR_OOM);
+  if (cudaMallocHost(&b->flags_h, sizeof(int)) != cudaSuccess) return fail(PCL_ERR_OOM);
+  *b->flags_h = 0;
   cudaMemsetAsync(b->scal_d, 0, sizeof(int) * 4, b->stream);
   cudaMemsetAsync(b->counters_d, 0, sizeof(int) * 2 * max_instances, b->stream);
   cudaMemsetAsync(b->totals_d, 0, sizeof(int) * 2 * max_instances, b->stream);
@@ -324,6 +332,7 @@ int pcl_batch_destroy(pcl_batch* b) {
   cudaFree(b->poll_d);
   cudaFree(b->staging_d);
   cudaFreeHost(b->ctl_h);
+  cudaFreeHost(b->flags_h);
   cudaStreamDestroy(b->stream);
   if (b->desc_base >= 0) batch_desc_release(b->desc_base, (int)b->slots.size());
   delete b;
@@ -335,7 +344,7 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   if (!vars && c->initial_condition != 1) return PCL_ERR_BADARG;
   int v = validate_control(c);
   if (v != PCL_OK) return v;
-  if (c->precision_mode != b->precision) return PCL_ERR_BADARG;
+  if (c->precision_mode != b->precision || c->num_equations != 3) return PCL_ERR_BADARG;
   int s = -1;
   for (int k = 0; k < (int)b->slots.size(); ++k)
     if (!b->slots[k].used) {
@@ -362,6 +371,7 @@ int pcl_batch_add(pcl_batch* b, const pcl_solver_control* c, const double* vars,
   GridDev g{};
   g.state = reinterpret_cast<double*>(mem);
   g.bufstride = 3 * plane;
+  g.neq = 3;
   g.rowm = reinterpret_cast<double*>(mem + off_tab);
   g.colm = g.rowm + rowm.size();
   g.ctl = reinterpret_cast<Ctl*>(mem + off_ctl);
@@ -481,7 +491,18 @@ int pcl_batch_step(pcl_batch* b, int nsteps) {
   b->launches += nsteps;
   b->steps += nsteps;
   BCK(cudaGetLastError());
+  // did a bounded wait give up during these steps?  (read and cleared in stream order)
+  BCK(cudaMemcpyAsync(b->flags_h, b->scal_d + 2, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemsetAsync(b->scal_d + 2, 0, sizeof(int), b->stream));
   BCK(cudaStreamSynchronize(b->stream));
+  return *b->flags_h ? PCL_ERR_TIMEOUT : PCL_OK;
+}
+
+int pcl_batch_inject_stall(pcl_batch* b, int slot, unsigned spin_limit) {
+  if (!b || slot < -1 || slot >= (int)b->slots.size() || b->precision != PCL_PREC_FP64) return PCL_ERR_BADARG;
+  b->stall_slot = slot;
+  b->spin_limit = spin_limit > 0 ? spin_limit : (1u << 24);
+  drop_graph(b);  // the captured launches carry the old view
   return PCL_OK;
 }
 

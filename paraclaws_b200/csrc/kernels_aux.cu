@@ -88,49 +88,52 @@ void launch_metric_check(const GridDev& g, cudaStream_t st) {
 // ------------------------------------------------------------------------------------------
 // ghost fill (the logic lives in pcl_ghost.cuh)
 // ------------------------------------------------------------------------------------------
+template <int N>
 __global__ void ghost_kernel(GridDev g, int force) {
   const Ctl* c = g.ctl;
   if (!force && c->ierr != 1) return;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid < ghost_items(g)) ghost_item(g, buffer(g, c->cur), tid);
+  if (tid < ghost_items(g)) ghost_item<N>(g, buffer(g, c->cur), tid);
 }
 
 void launch_ghost(const GridDev& g, int force, cudaStream_t st) {
   const int n = g.mx > g.my ? g.mx : g.my;
   const int total = 4 * 2 * n;
-  ghost_kernel<<<(total + 255) / 256, 256, 0, st>>>(g, force);
+  const int blocks = (total + 255) / 256;
+  if (g.neq == 1)
+    ghost_kernel<1><<<blocks, 256, 0, st>>>(g, force);
+  else if (g.neq == 4)
+    ghost_kernel<4><<<blocks, 256, 0, st>>>(g, force);
+  else
+    ghost_kernel<3><<<blocks, 256, 0, st>>>(g, force);
 }
 
 // ------------------------------------------------------------------------------------------
-// AoS (reference layout vars(3, -1:m+2, -1:m+2)) <-> SoA planes.  Upload writes all three
+// AoS (reference layout vars(neq, -1:m+2, -1:m+2)) <-> SoA planes.  Upload writes all three
 // rotation buffers so every buffer carries the initial corner ghosts, which the reference
 // never overwrites.
 // ------------------------------------------------------------------------------------------
 __global__ void upload_kernel(GridDev g, const double* __restrict__ aos) {
-  const int ni = g.mx + 4, nj = g.my + 4;
+  const int ni = g.mx + 4, nj = g.my + 4, ne = g.neq;
   const long long n = (long long)ni * nj;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     const int jj = (int)(c / ni), ii = (int)(c - (long long)jj * ni);
     const long long o = (long long)jj * g.pitch + ii;
-    const double h = aos[c * 3], hu = aos[c * 3 + 1], hv = aos[c * 3 + 2];
-    for (int b = 0; b < 3; ++b) {
-      buffer(g, b)[o] = h;
-      buffer(g, b)[o + g.plane] = hu;
-      buffer(g, b)[o + 2 * g.plane] = hv;
+    for (int p = 0; p < ne; ++p) {
+      const double v = aos[c * ne + p];
+      for (int b = 0; b < 3; ++b) buffer(g, b)[o + p * g.plane] = v;
     }
   }
 }
 
 __global__ void download_kernel(GridDev g, double* __restrict__ aos) {
-  const int ni = g.mx + 4, nj = g.my + 4;
+  const int ni = g.mx + 4, nj = g.my + 4, ne = g.neq;
   const long long n = (long long)ni * nj;
   const double* b = buffer(g, g.ctl->cur);
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
     const int jj = (int)(c / ni), ii = (int)(c - (long long)jj * ni);
     const long long o = (long long)jj * g.pitch + ii;
-    aos[c * 3] = b[o];
-    aos[c * 3 + 1] = b[o + g.plane];
-    aos[c * 3 + 2] = b[o + 2 * g.plane];
+    for (int p = 0; p < ne; ++p) aos[c * ne + p] = b[o + p * g.plane];
   }
 }
 

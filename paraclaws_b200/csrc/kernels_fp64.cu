@@ -24,22 +24,28 @@ constexpr int kYT = 128;   // columns of an eta-sweep CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 16;    // rows of an eta-sweep strip
 
-// MK values >= 16 select the generic equation-module path (GEN) with metric MK - 16.
-template <int NT, int LIM, bool SO, int MK>
+// A CTA sweeps R consecutive rows of one segment (blockIdx.y*R ..), strided by gridDim.y*R
+// when the grid has more rows than one launch's blocks cover.
+template <int NT, int LIM, bool SO, int MK, int R = 1, int OPT = 0>
 __global__ void __launch_bounds__(NT, kXMinBlocks) xsweep_fp64_kernel(GridDev g) {
   __shared__ XSmem<NT> S;
   if (g.ctl->done) return;
-  // one row per blockIdx.y, strided when the grid has more rows than gridDim.y allows
-  for (int j = 1 + blockIdx.y; j <= g.my; j += gridDim.y) {
-    xsweep_segment<NT, LIM, SO, MK % 16, (MK >= 16)>(g, j, 1 + blockIdx.x * (NT - 4), S);
-    if (j + gridDim.y <= g.my) __syncthreads();  // the shared arrays are reused by the next row
+  double smax = 0.0;
+  int bad = 0;
+  for (int jb = 1 + blockIdx.y * R; jb <= g.my; jb += gridDim.y * R) {
+    const int je = min(jb + R - 1, g.my);
+    for (int j = jb; j <= je; ++j) {
+      xsweep_segment<NT, LIM, SO, MK, OPT>(g, j, 1 + blockIdx.x * (NT - 4), S, smax, bad);
+      __syncthreads();  // the shared arrays are reused by the next row
+    }
   }
+  xsweep_finish<NT>(g, smax, bad, S);
 }
 
 template <int NTX, int STRIP, int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g) {
   if (g.ctl->done) return;
-  ysweep_strip<LIM, SO, MK % 16, (MK >= 16)>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
+  ysweep_strip<LIM, SO, MK>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
 }
 
 template <int LIM, bool SO, int MK>
@@ -65,10 +71,6 @@ void dispatch_lim(const GridDev& g, cudaStream_t st) {
 }
 template <template <int, bool, int> class F>
 void dispatch(const GridDev& g, cudaStream_t st) {
-  if (g.eq != PCL_EQ_SHALLOW_WATER) {  // generic modules: uniform grids (pcl_set_equation checks)
-    if (g.metric == kMetricUnit) return dispatch_lim<F, 16 + kMetricUnit>(g, st);
-    return dispatch_lim<F, 16 + kMetricTable>(g, st);
-  }
   if (g.metric == kMetricUnit) return dispatch_lim<F, kMetricUnit>(g, st);
   if (g.metric == kMetricMapped) return dispatch_lim<F, kMetricMapped>(g, st);
   return dispatch_lim<F, kMetricTable>(g, st);
@@ -83,8 +85,15 @@ struct YL {
 };
 }  // namespace
 
-void launch_xsweep_fp64(const GridDev& g, cudaStream_t st) { dispatch<XL>(g, st); }
-void launch_ysweep_fp64(const GridDev& g, cudaStream_t st) { dispatch<YL>(g, st); }
+// Modules other than the specialised shallow water run the generic sweeps (kernels_gen.cu).
+void launch_xsweep_fp64(const GridDev& g, cudaStream_t st) {
+  if (g.eq != PCL_EQ_SHALLOW_WATER) return launch_xsweep_gen(g, st);
+  dispatch<XL>(g, st);
+}
+void launch_ysweep_fp64(const GridDev& g, cudaStream_t st) {
+  if (g.eq != PCL_EQ_SHALLOW_WATER) return launch_ysweep_gen(g, st);
+  dispatch<YL>(g, st);
+}
 void launch_sweeps_fp64(const GridDev& g, cudaStream_t st) {
   launch_xsweep_fp64(g, st);
   launch_ysweep_fp64(g, st);

@@ -9,17 +9,22 @@
 namespace pcl {
 namespace mixed {
 
-template <int LIM, bool SO>
-__global__ void __launch_bounds__(NT) fused_mixed_kernel(GridDev g, int TY, int nstrips) {
+// INJ: the build for the test of the timeout path (mixed_item), launched only while a copy
+// stall is injected from the host (mixed_set_injection).
+template <int LIM, bool SO, bool INJ = false>
+__global__ void __launch_bounds__(NT) fused_mixed_kernel(GridDev g, int TY, int nstrips, int inj_row,
+                                                         unsigned probes) {
   __shared__ Smem S;
   if (g.ctl->done) return;
   init_ring(S);
   unsigned rows = 0;
-  mixed_item<LIM, SO, 2>(g, blockIdx.x % nstrips, blockIdx.x / nstrips, TY, S, rows);
+  mixed_item<LIM, SO, 2, INJ>(g, blockIdx.x % nstrips, blockIdx.x / nstrips, TY, S, rows, inj_row, probes);
 }
 
 struct Workspace {
   int ty;
+  int inj_row = -1;        // row whose bulk copy is not issued (-1: none)
+  unsigned probes = 0;     // probe limit of the waits in that build
 };
 
 }  // namespace mixed
@@ -49,24 +54,36 @@ void mixed_set_tile_rows(void* ws, int ty) {
   if (ws && ty >= 4) static_cast<mixed::Workspace*>(ws)->ty = ty;
 }
 
+void mixed_set_injection(void* ws, int row, unsigned probes) {
+  if (!ws) return;
+  auto* w = static_cast<mixed::Workspace*>(ws);
+  w->inj_row = row;
+  w->probes = probes > 0 ? probes : 1u;
+}
+
 namespace {
 template <int LIM, bool SO>
-void launch_t(const GridDev& g, int ty, cudaStream_t st) {
+void launch_t(const GridDev& g, const mixed::Workspace* w, cudaStream_t st) {
+  const int ty = w ? w->ty : 64;
   const int nstrips = (g.mx + mixed::TXI - 1) / mixed::TXI;
   const int nseg = (g.my + ty - 1) / ty;
-  mixed::fused_mixed_kernel<LIM, SO><<<nstrips * nseg, mixed::NT, 0, st>>>(g, ty, nstrips);
+  if (w && w->inj_row >= 0)
+    mixed::fused_mixed_kernel<LIM, SO, true><<<nstrips * nseg, mixed::NT, 0, st>>>(g, ty, nstrips, w->inj_row,
+                                                                                  w->probes);
+  else
+    mixed::fused_mixed_kernel<LIM, SO><<<nstrips * nseg, mixed::NT, 0, st>>>(g, ty, nstrips, -1, 0u);
 }
 }  // namespace
 
 void launch_sweeps_mixed(const GridDev& g, void* ws, cudaStream_t st) {
-  const int ty = ws ? static_cast<mixed::Workspace*>(ws)->ty : 64;
-  if (!g.second_order) return launch_t<0, false>(g, ty, st);
+  const auto* w = static_cast<const mixed::Workspace*>(ws);
+  if (!g.second_order) return launch_t<0, false>(g, w, st);
   switch (g.limiter) {
-    case 1: return launch_t<1, true>(g, ty, st);
-    case 2: return launch_t<2, true>(g, ty, st);
-    case 3: return launch_t<3, true>(g, ty, st);
-    case 4: return launch_t<4, true>(g, ty, st);
-    default: return launch_t<0, true>(g, ty, st);
+    case 1: return launch_t<1, true>(g, w, st);
+    case 2: return launch_t<2, true>(g, w, st);
+    case 3: return launch_t<3, true>(g, w, st);
+    case 4: return launch_t<4, true>(g, w, st);
+    default: return launch_t<0, true>(g, w, st);
   }
 }
 

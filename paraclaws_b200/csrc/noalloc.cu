@@ -14,6 +14,11 @@
 // so every call rewrites what the step reads before reading it (control block, tables, input
 // copy); two calls whose work overlaps on the GPU (different streams or devices of one process
 // that run at the same time on the same device) race on the array.
+//
+// The array's device address is looked up once per device and kept: it belongs to that device's
+// primary context and stays valid while the context lives.  A cudaDeviceReset on the device ends
+// the context, and the kept address with it: a process that resets a device must not call this
+// entry point on it afterwards.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -70,6 +75,25 @@ static int scratch_address(int device, double** out) {
   }
   *out = g_scratch_addr[device];
   return PCL_OK;
+}
+
+// True when every capacity of cells -1 .. m+2 and every interior face length ratio of the
+// uniform grid is exactly 1.0, computed from the tables with the sweeps' own expression
+// (pcl_fp64.cuh: capacity) without contraction, as the regular contexts' metric check does on
+// the device.  The sweeps then drop those identity operations (same bits, fewer instructions).
+static bool unit_metric(const std::vector<double>& rowm, const std::vector<double>& colm, int mx, int my,
+                        double area_scale) {
+  for (int j = -1; j <= my + 2; ++j)
+    for (int i = -1; i <= mx + 2; ++i) {
+      const double* r = &rowm[(size_t)(j + 1) * pcl::kRowMetrics];
+      const double* c = &colm[(size_t)(i + 1) * pcl::kColMetrics];
+      if ((r[0] * c[0] + r[1] * c[1]) / area_scale != 1.0) return false;
+    }
+  for (int j = 1; j <= my; ++j)
+    if (rowm[(size_t)(j + 1) * pcl::kRowMetrics + 2] != 1.0) return false;
+  for (int i = 1; i <= mx; ++i)
+    if (colm[(size_t)(i + 1) * pcl::kColMetrics + 2] != 1.0) return false;
+  return true;
 }
 
 static int status_code(int st) {
@@ -146,6 +170,7 @@ extern "C" int pcl_solve_dimensional_split_noalloc(const pcl_solver_control* c, 
 
   g.state = base;
   g.bufstride = 3 * plane;
+  g.neq = 3;
   g.rowm = base + kTableOffset;
   g.colm = base + kTableOffset + (long long)(my + 4) * pcl::kRowMetrics;
   g.ctl = reinterpret_cast<pcl::Ctl*>(base + kCtlOffset);
@@ -160,6 +185,7 @@ extern "C" int pcl_solve_dimensional_split_noalloc(const pcl_solver_control* c, 
   g.deta = deta;
   g.area_scale = dxi * deta;
   g.grav = c->grav;
+  g.metric = unit_metric(rowm, colm, mx, my, g.area_scale) ? pcl::kMetricUnit : pcl::kMetricTable;
 
   NA_CK(cudaMemcpyAsync(const_cast<double*>(g.rowm), rowm.data(), sizeof(double) * rowm.size(),
                         cudaMemcpyHostToDevice, st));

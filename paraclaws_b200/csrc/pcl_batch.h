@@ -45,6 +45,9 @@ struct BatchView {
   int item_ghosts;       // 1: the builds whose edge items fill ghost cells, 0: the builds
                          // whose finishing CTA fills them all
   unsigned spin_limit;   // bounded waits of eta items for their xi items
+  int* flags;            // device scalar: bit 0 set when any bounded wait of the launch gave up
+  int stall_slot;        // test of the timeout path (-1: off): the eta items of this slot wait
+                         // for one xi item more than the step has, so their wait runs out
 };
 
 void launch_batch_fp64(const BatchView& v, int grid, cudaStream_t st);

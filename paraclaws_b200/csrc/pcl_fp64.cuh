@@ -25,6 +25,7 @@ namespace pcl {
 // (solver/SMOD_approximate_Riemann_solvers.f90:186-190 takes maxval of |eig| over both cells).
 struct CellFlux {
   double f0, f1, f2, s;
+  bool ok;  // h, hu, hv inside the range of the shared-reciprocal quotients (kOptFastDiv)
 };
 
 // IEEE division with the zero-numerator case answered without dividing.  CUDA's correctly
@@ -52,22 +53,76 @@ __device__ __forceinline__ double div_neg_den(double a, double b) {  // quotient
   return z ? -a : q;
 }
 
-template <int DIR>
+// ---- correctly rounded quotients that share a denominator ----
+// Markstein's correction step (P. W. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990): when y = RN(1/b) and q is
+// within one ulp of a/b, the remainder r = a - b*q is exactly representable (one FMA gives it)
+// and RN(q + r*y) = RN(a/b).  q0 = RN(a*y) can be up to 1.5 ulp off, so one correction first
+// brings it within one ulp and a second gives the correctly rounded quotient: the same bits as
+// IEEE division, in one multiply and four FMAs per quotient after one reciprocal
+// (__drcp_rn, correctly rounded) per denominator.  The remainders are exact and nothing
+// underflows or overflows while a, b and a/b lie in [2^-960, 2^960] in magnitude; a = 0 takes
+// q0 = a*y, the exactly signed zero.  Callers establish the range once per cell (mag_ok) and
+// use IEEE division for cells outside it.
+struct Den {
+  double b, y;
+};
+__device__ __forceinline__ Den den_of(double b) { return Den{b, __drcp_rn(b)}; }
+__device__ __forceinline__ double quot(double a, const Den& d) {
+  const double q0 = __dmul_rn(a, d.y);
+  const double q1 = __fma_rn(__fma_rn(-q0, d.b, a), d.y, q0);
+  const double q2 = __fma_rn(__fma_rn(-q1, d.b, a), d.y, q1);
+  return a == 0.0 ? q0 : q2;
+}
+// |x| is 0 or in [2^-64, 2^64) (biased exponent 959 .. 1086)
+__device__ __forceinline__ bool mag_ok(double x) {
+  const unsigned e = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
+  return e - 959u <= 127u || x == 0.0;
+}
+// x > 0 and in [2^-64, 2^64): the sign bit sits above the exponent, so one compare does both
+__device__ __forceinline__ bool pos_ok(double x) { return ((unsigned)__double2hiint(x) >> 20) - 959u <= 127u; }
+
+// Sweep-kernel options (template bit mask, results identical for every value):
+//   kOptFastDiv  cell flux and HLL quotients from shared reciprocals (Markstein, above) for
+//                cells whose h, hu, hv pass pos_ok/mag_ok, with g in [2^-20, 2^20] (the host
+//                picks the build).  Every quotient of the flux and of the HLL solve then stays
+//                inside the method's range: a non-zero sum of two doubles is at least 2^-53
+//                times the smaller one, which bounds every non-zero flux below by 2^-426 and
+//                every non-zero HLL numerator by 2^-585, with |den| in [2^-34, 2^130], so all
+//                quotients lie in [2^-716, 2^356] and their remainders stay normal.
+//   kOptLimSat   the limiter ratio theta = up/|W|^2 is only divided out where the limiter
+//                function does not saturate (see limit_wave)
+enum : int { kOptFastDiv = 1, kOptLimSat = 2 };
+
+template <int DIR, int OPT = 0>
 __device__ __forceinline__ CellFlux cell_flux(double h, double hu, double hv, double g, int* bad) {
   const double n = DIR == 0 ? hu : hv;
   const double hh = h * h;
-  const double d1 = div_pos_den(n * n, hh);
-  const double d3 = div_pos_den(hu * hv, hh);
-  const double d4 = div_pos_den(hv, h);
-  const double d5 = div_pos_den(hu, h);
+  double d1, d3, d4, d5, d2;
+  bool fast = false;
+  if constexpr ((OPT & kOptFastDiv) != 0) fast = pos_ok(h) && mag_ok(hu) && mag_ok(hv);
+  if (fast) {
+    // h, |hu|, |hv| in [2^-64, 2^64) (or momenta 0): n/h is 0 or normal, so (2n)/h = 2*(n/h)
+    const Den rh = den_of(h), rhh = den_of(hh);
+    d1 = quot(n * n, rhh);
+    d3 = quot(hu * hv, rhh);
+    d4 = quot(hv, rh);
+    d5 = quot(hu, rh);
+    d2 = 2.0 * (DIR == 0 ? d5 : d4);
+  } else {
+    d1 = div_pos_den(n * n, hh);
+    d3 = div_pos_den(hu * hv, hh);
+    d4 = div_pos_den(hv, h);
+    d5 = div_pos_den(hu, h);
+    const double u = DIR == 0 ? d5 : d4;
+    // (2n)/h == 2*(n/h) exactly unless n/h is subnormal (scaling by 2 commutes with rounding);
+    // a branch, so the rare division is not evaluated for every cell
+    if (fabs(u) >= 0x1p-1000)
+      d2 = 2.0 * u;
+    else
+      d2 = div_pos_den(2.0 * n, h);
+  }
   const double un = DIR == 0 ? d5 : d4;
-  // (2n)/h == 2*(n/h) exactly unless n/h is subnormal (scaling by 2 commutes with rounding);
-  // a branch, so the rare division is not evaluated for every cell
-  double d2;
-  if (fabs(un) >= 0x1p-1000)
-    d2 = 2.0 * un;
-  else
-    d2 = div_pos_den(2.0 * n, h);
   const double gh = g * h;
   const double jn = -d1 + gh;
   const double jt = -d3;
@@ -78,34 +133,15 @@ __device__ __forceinline__ CellFlux cell_flux(double h, double hu, double hv, do
   c.f1 = DIR == 0 ? fnorm : ftran;
   c.f2 = DIR == 0 ? ftran : fnorm;
   c.s = fabs(un) + sqrt(gh);
+  c.ok = fast;
   // getJakobi's NaN trap (SMOD_jakobian.f90:55-70) and dgeev's complex-eigenvalue abort
-  // (utility/SMOD_eigenvalue_problem.f90:72-83, h < 0) become status bits.
-  if (isnan(jn) || isnan(d2) || isnan(jt) || isnan(d4) || isnan(d5)) *bad |= kStatusNaN;
-  if (h < 0.0) *bad |= kStatusNegDepth;
-  return c;
-}
-
-// Flux and wave-speed bound of a cell for any equation module (pcl_equations.h): J(q) from the
-// module, f = J.q in BLAS dgemv order (((0 + q1*J(:,1)) + q2*J(:,2)) + q3*J(:,3)), s = max |eig|.
-template <int DIR>
-__device__ __forceinline__ CellFlux cell_flux_generic(int module, double h, double hu, double hv, const double* prm,
-                                                      int* bad) {
-  const double q[3] = {h, hu, hv};
-  double J[9];
-  if (pcl_eq_jacobian(module, DIR + 1, q, prm, J)) *bad |= kStatusNaN;
-  double f[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const double temp = q[c];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) f[r] = f[r] + temp * J[c * 3 + r];
+  // (utility/SMOD_eigenvalue_problem.f90:72-83, h < 0) become status bits.  A cell in the
+  // fast range has h > 0 and finite Jacobian entries.
+  if (!fast) {
+    if (isnan(jn) || isnan(d2) || isnan(jt) || isnan(d4) || isnan(d5)) *bad |= kStatusNaN;
+    if (h < 0.0) *bad |= kStatusNegDepth;
   }
-  double lam[3];
-  if (pcl_eq_eigenvalues(module, DIR + 1, q, prm, lam)) *bad |= kStatusNegDepth;
-  double s = fabs(lam[0]);
-  s = fabs(lam[1]) > s ? fabs(lam[1]) : s;
-  s = fabs(lam[2]) > s ? fabs(lam[2]) : s;
-  return CellFlux{f[0], f[1], f[2], s};
+  return c;
 }
 
 // HLL two-wave solve at one interface (SMOD_approximate_Riemann_solvers.f90:189-224):
@@ -116,6 +152,7 @@ struct Waves {
   double w1[3], w2[3];
 };
 
+template <int OPT = 0>
 __device__ __forceinline__ double hll(const double qL[3], const CellFlux& fL, const double qR[3],
                                       const CellFlux& fR, Waves& W) {
   const double smax = fmax(fL.s, fR.s);
@@ -124,11 +161,22 @@ __device__ __forceinline__ double hll(const double qL[3], const CellFlux& fL, co
     const double den = (kUdPrecision + s1) - smax;
     const double fl[3] = {fL.f0, fL.f1, fL.f2};
     const double fr[3] = {fR.f0, fR.f1, fR.f2};
+    double num[3];
+#pragma unroll
+    for (int me = 0; me < 3; ++me) num[me] = ((fr[me] - fl[me]) - smax * qR[me]) + s1 * qL[me];
+    double qs[3];
+    if ((OPT & kOptFastDiv) != 0 && fL.ok && fR.ok) {  // both cells in range: one reciprocal
+      const Den d = den_of(den);
+#pragma unroll
+      for (int me = 0; me < 3; ++me) qs[me] = quot(num[me], d);
+    } else {
+#pragma unroll
+      for (int me = 0; me < 3; ++me) qs[me] = div_neg_den(num[me], den);
+    }
 #pragma unroll
     for (int me = 0; me < 3; ++me) {
-      const double qs = div_neg_den(((fr[me] - fl[me]) - smax * qR[me]) + s1 * qL[me], den);
-      W.w1[me] = qs - qL[me];
-      W.w2[me] = qR[me] - qs;
+      W.w1[me] = qs[me] - qL[me];
+      W.w2[me] = qR[me] - qs[me];
     }
     return smax;
   }
@@ -158,7 +206,14 @@ __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
 // original waves at k and k+1, taken before wave k is limited in place.
 //   upstream = lambda_p > 0 ? W_{k-1}.W_k : W_k.W_{k+1};  theta = upstream / |W_k|^2
 //   W~ = |W_k|^2 <= eps ? W_k : phi(theta) * W_k
-template <int LIM>
+//
+// kOptLimSat leaves the division out where phi is known without it (wn2 > eps > 0 here):
+//   up >= K*wn2 means theta >= K, where phi saturates: minmod (K = 1) and superbee (K = 2) give
+//     phi = K, MC (K = 4, a power of two so K*wn2 is exact) gives 2; van Leer never saturates;
+//   up < -2^-900 with wn2 < 2^100 means theta is a negative normal number (it cannot underflow
+//     to -0), where every limiter gives +0 (fmax(0, negative) = +0; van Leer: (t + |t|) = +0).
+// Everything else divides, so phi has the same bits either way.
+template <int LIM, int OPT = 0>
 __device__ __forceinline__ void limit_wave(const double wm[3], const double w[3], const double wp[3],
                                            bool lambda_pos, double out[3]) {
   const double wn2 = dot3(w, w);
@@ -169,7 +224,19 @@ __device__ __forceinline__ void limit_wave(const double wm[3], const double w[3]
     return;
   }
   const double up = lambda_pos ? dot3(wm, w) : dot3(w, wp);
-  const double phi = limiter_phi<LIM>(div_pos_den(up, wn2));
+  double phi;
+  if constexpr ((OPT & kOptLimSat) != 0) {
+    constexpr double K = LIM == 1 ? 1.0 : LIM == 2 ? 2.0 : 4.0;
+    constexpr double SAT = LIM == 1 ? 1.0 : 2.0;
+    if (LIM != 3 && up >= K * wn2)
+      phi = SAT;
+    else if (up < -0x1p-900 && wn2 < 0x1p100)
+      phi = 0.0;
+    else
+      phi = limiter_phi<LIM>(div_pos_den(up, wn2));
+  } else {
+    phi = limiter_phi<LIM>(div_pos_den(up, wn2));
+  }
   out[0] = phi * w[0];
   out[1] = phi * w[1];
   out[2] = phi * w[2];

@@ -3,26 +3,36 @@
 // over item indices so a whole kernel or one CTA of a batched kernel can run it.
 // Items: 4 sides x 2 layers x max(m_xi, m_eta) positions; corners are never written.
 // Code 1 (BC_USER, which aborts in the reference) is a reflective wall here: the two ghost
-// layers mirror the two nearest interior cells with the normal momentum negated.
+// layers mirror the two nearest interior cells with the normal momentum (or velocity) of the
+// equation module negated (pcl_eq_wall_component); a module without one mirrors every component.
+// N: the context's number of equations (planes).
 #pragma once
 #include <cuda_runtime.h>
 
+#include "pcl_equations.h"
 #include "pcl_types.h"
 
 namespace pcl {
 
 __device__ __forceinline__ int ghost_items(const GridDev& g) { return 8 * max(g.mx, g.my); }
 
-// One ghost cell's three values and where they go (plane 0; plane p at dst + p * plane).
+// One ghost cell's N values and where they go (plane 0; plane p at dst + p * plane).
+template <int N = 3>
 struct GhostVal {
   double* dst;
-  double v[3];
+  double v[N];
 };
 
+// the component a wall negates on the xi (dir 1) or eta (dir 2) sides; -1: none
+__device__ __forceinline__ int wall_component(const GridDev& g, int dir) {
+  return g.eq == PCL_EQ_SHALLOW_WATER ? dir : pcl_eq_wall_component(g.eq, dir);
+}
+
 // Loads only: no ghost item reads a cell that another one writes (sources are interior cells
-// and the metric tables), so the three planes of an item are all loaded before any is stored
+// and the metric tables), so the planes of an item are all loaded before any is stored
 // (one memory round trip per item, not one per plane).  Returns false where it writes nothing.
-__device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid, GhostVal& o) {
+template <int N = 3>
+__device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid, GhostVal<N>& o) {
   const int mx = g.mx, my = g.my;
   const int n = max(mx, my);
   const int side = tid / (2 * n);
@@ -44,8 +54,9 @@ __device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid
     const double x1 = __ldg(g.colm + (i1 + 1) * kColMetrics + 3);
     const double x2 = __ldg(g.colm + (i2 + 1) * kColMetrics + 3);
     o.dst = b + (long long)(j + 1) * P + (i + 1);
+    const int wc = bc == 1 ? wall_component(g, 1) : -1;
 #pragma unroll
-    for (int me = 0; me < 3; ++me) {
+    for (int me = 0; me < N; ++me) {
       const double* p = b + me * g.plane + (long long)(j + 1) * P;
       double v;
       if (bc == 2) {
@@ -59,7 +70,7 @@ __device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid
         const double xb = side == 0 ? x2 : x1;
         v = p[i1 + 1] + (yb - ya) / (xb - xa) * (xg - x1);
       } else {
-        v = me == 1 ? -p[im + 1] : p[im + 1];
+        v = me == wc ? -p[im + 1] : p[im + 1];
       }
       o.v[me] = v;
     }
@@ -74,8 +85,9 @@ __device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid
     const double y1 = __ldg(g.rowm + (j1 + 1) * kRowMetrics + 3);
     const double y2 = __ldg(g.rowm + (j2 + 1) * kRowMetrics + 3);
     o.dst = b + (long long)(j + 1) * P + (i + 1);
+    const int wc = bc == 1 ? wall_component(g, 2) : -1;
 #pragma unroll
-    for (int me = 0; me < 3; ++me) {
+    for (int me = 0; me < N; ++me) {
       const double* p = b + me * g.plane + (i + 1);
       double v;
       if (bc == 2) {
@@ -87,7 +99,7 @@ __device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid
         const double yb = side == 2 ? y2 : y1;
         v = p[(long long)(j1 + 1) * P] + (vb - va) / (yb - ya) * (yg - y1);
       } else {
-        v = me == 2 ? -p[(long long)(jm + 1) * P] : p[(long long)(jm + 1) * P];
+        v = me == wc ? -p[(long long)(jm + 1) * P] : p[(long long)(jm + 1) * P];
       }
       o.v[me] = v;
     }
@@ -95,15 +107,16 @@ __device__ __forceinline__ bool ghost_value(const GridDev& g, double* b, int tid
   return true;
 }
 
-__device__ __forceinline__ void ghost_store(const GridDev& g, const GhostVal& o) {
-  o.dst[0] = o.v[0];
-  o.dst[g.plane] = o.v[1];
-  o.dst[2 * g.plane] = o.v[2];
+template <int N = 3>
+__device__ __forceinline__ void ghost_store(const GridDev& g, const GhostVal<N>& o) {
+#pragma unroll
+  for (int me = 0; me < N; ++me) o.dst[me * g.plane] = o.v[me];
 }
 
+template <int N = 3>
 __device__ __forceinline__ void ghost_item(const GridDev& g, double* b, int tid) {
-  GhostVal o;
-  if (ghost_value(g, b, tid, o)) ghost_store(g, o);
+  GhostVal<N> o;
+  if (ghost_value<N>(g, b, tid, o)) ghost_store<N>(g, o);
 }
 
 // Ghost cells next to a block of interior cells [i0, i1] x [j0, j1] of buffer b that the calling

@@ -19,6 +19,9 @@ enum TimeOp : int {
 };
 
 void launch_sweeps_fp64(const GridDev& g, cudaStream_t st);
+// the FP64 sweeps of the equation modules other than the specialised shallow water
+void launch_xsweep_gen(const GridDev& g, cudaStream_t st);
+void launch_ysweep_gen(const GridDev& g, cudaStream_t st);
 void launch_xsweep_fp64(const GridDev& g, cudaStream_t st);
 void launch_ysweep_fp64(const GridDev& g, cudaStream_t st);
 void launch_timectl(const GridDev& g, int op, int arg, double value, cudaStream_t st);

@@ -8,5 +8,8 @@ namespace pcl {
 int mixed_create(const GridDev& g, cudaStream_t st, void** ws);
 void mixed_free(void* ws);
 void mixed_set_tile_rows(void* ws, int ty);   // rows per work item of the fused kernel
+// test of the timeout path: the bulk copy of `row` is not issued and waits give up after
+// `probes` probes (row < 0: off)
+void mixed_set_injection(void* ws, int row, unsigned probes);
 void launch_sweeps_mixed(const GridDev& g, void* ws, cudaStream_t st);
 }  // namespace pcl

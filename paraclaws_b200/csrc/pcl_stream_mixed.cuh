@@ -161,8 +161,12 @@ __device__ __forceinline__ WF load_wf(const Smem& S, int s) {
 // changes no arithmetic.
 // G is GridDev or any descriptor with its fields ctl, grav, mx, my, pitch, plane, state and
 // bufstride (the batch keeps a compact one in constant memory).
-template <int LIM, bool SO, int UNROLL = 1, class G>
-__device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int TY, Smem& S, unsigned& rows) {
+// INJ (a separate build, used only by the test of the timeout path): the bulk copy of row
+// inj_row is never issued, so the wait for it runs out after `probes` probes; the copies that
+// were issued are drained as after any timeout.
+template <int LIM, bool SO, int UNROLL = 1, bool INJ = false, class G>
+__device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int TY, Smem& S, unsigned& rows,
+                                           int inj_row = -1, unsigned probes = 1u << 22) {
   Ctl* ctl = g.ctl;
   const int t = threadIdx.x;
   const int cur = ctl->cur;
@@ -185,6 +189,7 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
 
   const unsigned base = rows;
   auto issue = [&](int row, int slot) {
+    if (INJ && row == inj_row) return;
     if (t == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&S.bar[slot], 3u * ncopy * 8u);
@@ -220,7 +225,8 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
       issue(jr + AHEAD, (kk + AHEAD) & (RING - 1));
       issued++;
     }
-    const bool ok = mbar_wait_bounded(&S.bar[slot], (kk / RING) & 1u);
+    const bool ok = INJ ? mbar_wait_bounded(&S.bar[slot], (kk / RING) & 1u, probes)
+                        : mbar_wait_bounded(&S.bar[slot], (kk / RING) & 1u);
     if (__syncthreads_or(!ok)) {
       timed_out = true;
       break;
@@ -334,7 +340,12 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
 
   if (timed_out && t == 0) {
     // drain the copies this CTA still has in flight before its shared memory goes away
-    for (int k = consumed; k < issued; ++k) mbar_wait_bounded(&S.bar[(base + k) & (RING - 1)], ((base + k) / RING) & 1u);
+    for (int k = consumed; k < issued; ++k) {
+      if (INJ)
+        mbar_wait_bounded(&S.bar[(base + k) & (RING - 1)], ((base + k) / RING) & 1u, probes);
+      else
+        mbar_wait_bounded(&S.bar[(base + k) & (RING - 1)], ((base + k) / RING) & 1u);
+    }
   }
   rows = base + issued;
   // eta-sweep speeds count only real columns

@@ -45,11 +45,23 @@ struct XSmem {
   double sq[3][NT], sf[3][NT], ss[NT], sk[NT];
   double sw1[3][NT], sw2[3][NT], ss2[NT], sft[3][NT];
   double red[NT / 32];
+  bool sok[NT];  // kOptFastDiv: the cell is in the range of the shared-reciprocal quotients
 };
 
-// GEN: a module other than the specialised shallow water (g.eq, pcl_equations.h)
-template <int NT, int LIM, bool SO, int MK = kMetricTable, bool GEN = false>
-__device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S) {
+// End of an xi-sweep CTA: the wave-speed maximum and the status bits of all its rows.
+template <int NT>
+__device__ __forceinline__ void xsweep_finish(const GridDev& g, double smax, int bad, XSmem<NT>& S) {
+  block_max_to<NT>(const_cast<unsigned long long*>(&g.ctl->smax_x), smax, S.red);
+  if (bad) atomicOr(&g.ctl->status, bad);
+}
+
+// The specialised shallow-water module (other modules: pcl_sweeps_gen.cuh).  OPT: the kOpt*
+// mask of pcl_fp64.cuh (same results for every value).  The row's wave-speed maximum is
+// folded into smax_acc and its status bits into bad_acc; the caller reduces them over the CTA
+// once for all the rows it sweeps (xsweep_finish).
+template <int NT, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
+__device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S, double& smax_acc,
+                                               int& bad_acc) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   const Ctl* ctl = g.ctl;
   constexpr int L = NT - 4;
@@ -70,7 +82,6 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
   auto& sw2 = S.sw2;
   auto& ss2 = S.ss2;
   auto& sft = S.sft;
-  auto& red = S.red;
 
   // phase A: per-cell flux J.q, wave-speed bound and capacity
   int bad = 0;
@@ -79,11 +90,12 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
     if (c <= mx + 2) {
       const double h = q0[c + 1], hu = q1[c + 1], hv = q2[c + 1];
       int cb = 0;
-      const CellFlux F = GEN ? cell_flux_generic<0>(g.eq, h, hu, hv, g.eqp, &cb) : cell_flux<0>(h, hu, hv, g.grav, &cb);
+      const CellFlux F = cell_flux<0, OPT>(h, hu, hv, g.grav, &cb);
       if (c <= mx + 1) bad |= cb;  // getJakobi runs on cells -1 .. m_xi+1 in the xi sweep
       sq[0][t] = h; sq[1][t] = hu; sq[2][t] = hv;
       sf[0][t] = F.f0; sf[1][t] = F.f1; sf[2][t] = F.f2;
       ss[t] = F.s;
+      if constexpr ((OPT & kOptFastDiv) != 0) S.sok[t] = F.ok;
       if constexpr (MP)
         sk[t] = __ldg(g.kap + row + c + 1);
       else if constexpr (!UM)
@@ -101,9 +113,10 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
     if (k <= mx + 1) {
       const double qL[3] = {sq[0][t], sq[1][t], sq[2][t]};
       const double qR[3] = {sq[0][t + 1], sq[1][t + 1], sq[2][t + 1]};
-      const CellFlux FL = {sf[0][t], sf[1][t], sf[2][t], ss[t]};
-      const CellFlux FR = {sf[0][t + 1], sf[1][t + 1], sf[2][t + 1], ss[t + 1]};
-      s2 = hll(qL, FL, qR, FR, W);
+      CellFlux FL = {sf[0][t], sf[1][t], sf[2][t], ss[t]};
+      CellFlux FR = {sf[0][t + 1], sf[1][t + 1], sf[2][t + 1], ss[t + 1]};
+      if constexpr ((OPT & kOptFastDiv) != 0) FL.ok = S.sok[t], FR.ok = S.sok[t + 1];
+      s2 = hll<OPT>(qL, FL, qR, FR, W);
       smax = s2;
     } else {
 #pragma unroll
@@ -116,8 +129,8 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
     }
     ss2[t] = s2;
   }
-  block_max_to<NT>(const_cast<unsigned long long*>(&g.ctl->smax_x), smax, red);
-  if (bad) atomicOr(&g.ctl->status, bad);
+  smax_acc = fmax(smax_acc, smax);
+  bad_acc |= bad;
   __syncthreads();
 
   // phase C: correction flux at interface k = i0+t (slot t+1); limited for 1 <= k <= m_xi,
@@ -139,8 +152,8 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
             const double w1p[3] = {sw1[0][s + 1], sw1[1][s + 1], sw1[2][s + 1]};
             const double w2m[3] = {sw2[0][s - 1], sw2[1][s - 1], sw2[2][s - 1]};
             const double w2p[3] = {sw2[0][s + 1], sw2[1][s + 1], sw2[2][s + 1]};
-            limit_wave<LIM>(w1m, w1, w1p, false, a);  // lambda_1 = -s2 <= 0
-            limit_wave<LIM>(w2m, w2, w2p, s2 > 0.0, b);
+            limit_wave<LIM, OPT>(w1m, w1, w1p, false, a);  // lambda_1 = -s2 <= 0
+            limit_wave<LIM, OPT>(w2m, w2, w2p, s2 > 0.0, b);
           } else {
 #pragma unroll
             for (int me = 0; me < 3; ++me) {
@@ -193,7 +206,7 @@ struct YCell {
   double lr;  // mapped grids: length ratio of the eta face below the cell
 };
 
-template <int LIM, bool SO, bool UM>
+template <int LIM, bool SO, bool UM, int OPT = 0>
 __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, const Waves& Wp, double s2,
                                             bool limited, double dtod, double kl, double kr, double ft[3]) {
   const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, kl, kr);
@@ -203,8 +216,8 @@ __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, con
   }
   double a[3], b[3];
   if (LIM != 0 && limited) {
-    limit_wave<LIM>(Wm.w1, W.w1, Wp.w1, false, a);
-    limit_wave<LIM>(Wm.w2, W.w2, Wp.w2, s2 > 0.0, b);
+    limit_wave<LIM, OPT>(Wm.w1, W.w1, Wp.w1, false, a);
+    limit_wave<LIM, OPT>(Wm.w2, W.w2, Wp.w2, s2 > 0.0, b);
   } else {
 #pragma unroll
     for (int me = 0; me < 3; ++me) {
@@ -216,7 +229,7 @@ __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, con
   for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
 }
 
-template <int LIM, bool SO, int MK = kMetricTable, bool GEN = false>
+template <int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
 __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   Ctl* ctl = g.ctl;
@@ -252,8 +265,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     c.q[1] = src[o + g.plane];
     c.q[2] = src[o + 2 * g.plane];
     int cb = 0;
-    c.F = GEN ? cell_flux_generic<1>(g.eq, c.q[0], c.q[1], c.q[2], g.eqp, &cb)
-              : cell_flux<1>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
+    c.F = cell_flux<1, OPT>(c.q[0], c.q[1], c.q[2], g.grav, &cb);
     if (jj <= my + 1) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
     if constexpr (MP) {
       c.kap = __ldg(g.kap + o);
@@ -269,7 +281,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
       for (int me = 0; me < 3; ++me) W.w1[me] = W.w2[me] = 0.0;
       return 0.0;
     }
-    const double s2 = hll(L.q, L.F, R.q, R.F, W);
+    const double s2 = hll<OPT>(L.q, L.F, R.q, R.F, W);
     smax = fmax(smax, s2);
     return s2;
   };
@@ -290,12 +302,12 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     s0 = iface(j0, cm1, cA, W0);
     load(j0 + 1, cB);
     s1 = iface(j0 + 1, cA, cB, W1);
-    if constexpr (SO) y_corr_flux<LIM, SO, UM>(Wm, W0, W1, s0, true, dtod, cm1.kap, cA.kap, ft0);
+    if constexpr (SO) y_corr_flux<LIM, SO, UM, OPT>(Wm, W0, W1, s0, true, dtod, cm1.kap, cA.kap, ft0);
   }
   for (int jj = j0; jj <= j1; ++jj) {
     load(jj + 2, cC);
     s2w = iface(jj + 2, cB, cC, W2);
-    if constexpr (SO) y_corr_flux<LIM, SO, UM>(W0, W1, W2, s1, jj + 1 <= my, dtod, cA.kap, cB.kap, ft1);
+    if constexpr (SO) y_corr_flux<LIM, SO, UM, OPT>(W0, W1, W2, s1, jj + 1 <= my, dtod, cA.kap, cB.kap, ft1);
     const double kap = (SO || UM || MP) ? cA.kap : capacity(g.rowm, g.colm, ic, jj, g.area_scale);
     const double gl = MP ? cA.lr : gam, gr = MP ? cB.lr : gam;  // faces below and above the cell
     const double dtk = UM ? dtod : dtod / kap;

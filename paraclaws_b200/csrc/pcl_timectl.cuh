@@ -79,6 +79,9 @@ __device__ __forceinline__ void finalize_solve(Ctl* c, const GridDev& g) {
     ok = c->CFL_target / c->CFL >= c->shrink;
   }
   c->cfl_y = cfl_local;
+  // A bounded wait that gave up (kStatusTimeout) voids the attempt: some of its cells were never
+  // written, so the eta-swept buffer must not become current.  The host sees the status.
+  if (__ldcg(&c->status) & kStatusTimeout) ok = false;
   c->ierr = ok ? 1 : -1;
   if (ok) c->cur = c->cur == 0 ? 2 : c->cur - 1;  // the eta-swept buffer becomes current
   c->smax_x = 0ull;
@@ -106,6 +109,12 @@ __device__ __forceinline__ void full_step(Ctl* c, const GridDev& g) {
   }
   const double dt_used = c->dt;
   finalize_solve(c, g);
+  if (__ldcg(&c->status) & kStatusTimeout) {  // void attempt: no time update, no ghost fill, no log
+    c->ierr = 0;
+    reset_cfl(c);
+    refresh_done(c);
+    return;
+  }
   const double cfl = c->CFL;
   bool ok = true;
   if (c->ierr < 0) {

@@ -1,10 +1,10 @@
 // pcl_types.h -- host/device shared types of the paraclaws_b200 CUDA path.
 //
 // Device state of one grid ("instance"):
-//   * three state buffers (rotation: current / x-swept / y-swept), each three SoA planes
-//     h, hu, hv of (m_eta+4) rows x pitch doubles; cell (i, j) of the reference's 1-based
-//     padded block (i, j = -1 .. m+2) sits at plane[(j+1)*pitch + (i+1)].  pitch is a multiple
-//     of 32 doubles so every row starts on a 256-byte boundary.
+//   * three state buffers (rotation: current / x-swept / y-swept), each num_equations SoA
+//     planes (shallow water: h, hu, hv) of (m_eta+4) rows x pitch doubles; cell (i, j) of the
+//     reference's 1-based padded block (i, j = -1 .. m+2) sits at plane[(j+1)*pitch + (i+1)].
+//     pitch is a multiple of 32 doubles so every row starts on a 256-byte boundary.
 //   * per-row and per-column mesh tables (uniform mapping: the capacity kappa(i,j) is rebuilt
 //     in-kernel from them in the reference's operation order);
 //   * a control block: the reference's time_control (time_control/MOD_time_control.f90:16-66)
@@ -83,7 +83,7 @@ struct Ctl {
 // Everything a sweep kernel needs about one grid.
 struct GridDev {
   double* state;             // 3 state buffers; plane p of buffer b at state + b*bufstride + p*plane
-  long long bufstride;       // doubles per buffer (3 planes)
+  long long bufstride;       // doubles per buffer (neq planes)
   const double* rowm;        // (m_eta+4) x kRowMetrics
   const double* colm;        // (m_xi+4) x kColMetrics
   Ctl* ctl;
@@ -93,7 +93,9 @@ struct GridDev {
   int second_order, limiter; // limiter 0: unlimited correction; 1..4 by code
   int metric;                // kMetric*
   int user_bc;               // 1: sides coded 1 are filled by the host's user hook, not the wall
-  int eq;                    // equation module (pcl_equations.h); 0: the specialised shallow water
+  int eq;                    // equation module (pcl_equations.h); 0: the specialised shallow water,
+                             // -1: none chosen yet (contexts of num_equations != 3)
+  int neq;                   // planes per buffer: num_equations (3 for every path but the generic one)
   double eqp[2];             // its parameters (shallow water: g)
   double dxi, deta, area_scale /* d_xi*d_eta */, grav;
   // kMetricMapped only: per-cell metrics, cell (i, j) at [(j+1)*pitch + (i+1)]

@@ -21,7 +21,7 @@ from typing import Deque, Dict, List, Optional
 
 import numpy as np
 
-from ._lib import PCL_ERR_FULL
+from ._lib import PCL_ERR_FULL, PCL_ERR_TIMEOUT
 from .batch import Batch, autotune
 from .control import ControlSettings, CustomSettings, PRECISION_FP64, dam_break_control
 from . import ic
@@ -59,8 +59,8 @@ class Result:
 def poisson_requests(n: int, rate: float, seed: int, side_lo: int = 128, side_hi: int = 2048,
                      t_end: tuple = (0.1, 1.0), limiter: int = 1, precision: int = PRECISION_FP64) -> List[Request]:
     """n dam-break requests with Poisson arrivals (rate per second), grid side log-uniform in
-    [side_lo, side_hi] (multiple of 32), end time U(t_end) and a seeded dam (radius, height
-    ratio, centre offset)."""
+    [side_lo, side_hi] (multiple of 32), end time U(t_end), a seeded dam (radius, height ratio,
+    centre offset) and reflective walls."""
     rng = np.random.Generator(np.random.PCG64(seed))
     gaps = rng.exponential(1.0 / rate, size=n)
     arrivals = np.cumsum(gaps) - gaps[0]
@@ -69,7 +69,7 @@ def poisson_requests(n: int, rate: float, seed: int, side_lo: int = 128, side_hi
     for k in range(n):
         te = float(rng.uniform(*t_end))
         p = ic.seeded_dam_params(seed * 100003 + k, offset=0.25)
-        c = dam_break_control(sides[k], limiter=limiter, bc=2, time_final=te)
+        c = dam_break_control(sides[k], limiter=limiter, bc=1, time_final=te)
         cu = CustomSettings(precision_mode=precision, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out,
                             dam_x0=p.x0, dam_y0=p.y0)
         out.append(Request(k, c, cu, float(arrivals[k])))
@@ -84,6 +84,7 @@ class ServeReport:
     peak_bytes: int
     peak_active: int
     steps: int
+    not_arrived: int = 0     # requests whose arrival time lay beyond the wall-clock limit
 
     def percentile(self, q: float) -> float:
         lat = sorted(r.latency for r in self.results)
@@ -104,6 +105,8 @@ class ServeReport:
             "peak_active": self.peak_active,
             "steps": self.steps,
             "errors": sum(1 for r in self.results if r.status != 0),
+            "timed_out": sum(1 for r in self.results if r.status == PCL_ERR_TIMEOUT),
+            "not_arrived": self.not_arrived,
         }
 
 
@@ -186,4 +189,18 @@ class SolveServer:
                 self.batch.remove(slot)
                 self.in_use -= need
         wall = clock() - t0
-        return ServeReport(sorted(results, key=lambda r: r.rid), wall, cell_updates, peak_bytes, peak_active, steps)
+        # max_wall ran out: every request still in flight or waiting is answered with a timeout, its
+        # latency the time it had waited so far (a lower bound), so percentiles and the error count
+        # include the requests that took longest.  Requests that had not arrived yet are left out.
+        for slot in list(self.active):
+            r, adm, need = self.active.pop(slot)
+            st = self.batch.stats(slot)
+            results.append(Result(r.rid, r.arrival, adm, wall, st.accepted, r.control.m_xi * r.control.m_eta,
+                                  PCL_ERR_TIMEOUT))
+            self.batch.remove(slot)
+            self.in_use -= need
+        while arrived:
+            r = arrived.popleft()
+            results.append(Result(r.rid, r.arrival, wall, wall, 0, r.control.m_xi * r.control.m_eta, PCL_ERR_TIMEOUT))
+        return ServeReport(sorted(results, key=lambda r: r.rid), wall, cell_updates, peak_bytes, peak_active, steps,
+                           not_arrived=len(pending) - i)

@@ -98,7 +98,7 @@ class Solver:
         h = C.c_void_p()
         _lib.check(self.L.pcl_create(C.byref(self.c), int(device), C.byref(h)), "pcl_create")
         self.h = h
-        self.shape = (control.m_eta + 4, control.m_xi + 4, 3)
+        self.shape = (control.m_eta + 4, control.m_xi + 4, int(control.number_of_equations))
 
     # -- lifecycle --
     def close(self) -> None:

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory (run once, in the container that has the
 reference checked out; the fixtures are committed and the tests never read the reference).
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 
 1. control.in / custom.in written by the reference's own input generator (write_input.py with
    control_settings.py of the project root and of examples/2D_dam_break/cartesian).
@@ -117,7 +117,9 @@ def tiny_runs() -> None:
 
 
 if __name__ == "__main__":
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    ref = Path(sys.argv[1])
     reference_inputs(ref)
     hll_kats()
     tiny_runs()

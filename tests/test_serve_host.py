@@ -172,3 +172,25 @@ def test_poisson_requests_are_seeded_and_in_range():
     long = serve.poisson_requests(4000, rate=5.0, seed=1)
     gaps = np.diff([r.arrival for r in long])
     assert abs(gaps.mean() - 0.2) < 0.02
+
+
+def test_wall_limit_answers_unfinished_requests_with_a_timeout(fake, monkeypatch):
+    """When max_wall runs out, requests still running or queued get a timeout result (their
+    latency so far), so the percentiles and the error count include them; requests that had
+    not arrived are counted apart."""
+    monkeypatch.setattr(FakeBatch, "step_seconds", 0.002)
+    sides = [2048, 2048, 64, 64]
+    # budget for one large instance: the second large one and the small ones queue behind it
+    srv = serve.SolveServer(budget_bytes=2048 * 2048 * 100 * 1.5, max_slots=8, steps_per_tick=4)
+    reqs = _requests(sides) + _requests([64], [30.0])
+    reqs[-1].rid = 4
+    rep = srv.run(reqs, max_wall=0.05)
+    srv.close()
+    by = {r.rid: r for r in rep.results}
+    assert sorted(by) == [0, 1, 2, 3], "every arrived request has a result"
+    assert by[0].status == serve.PCL_ERR_TIMEOUT and by[0].accepted > 0  # was running
+    assert by[1].status == serve.PCL_ERR_TIMEOUT and by[1].accepted == 0  # never admitted
+    s = rep.summary()
+    assert s["timed_out"] == 4 and s["errors"] == 4 and s["not_arrived"] == 1
+    assert s["p99_s"] >= 0.05 - 1e-3
+    assert FakeBatch.created[-1].slots == {}, "timed-out instances are removed from the batch"

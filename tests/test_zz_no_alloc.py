@@ -40,7 +40,7 @@ def _planes(q, ld):
     return p
 
 
-def _noalloc_step(c, filled, ld, dt, out_fill=0.0):
+def _noalloc_step(c, filled, ld, dt, out_fill=0.0, stream=None):
     import torch
     L = _lib.load()
     d_in = torch.from_numpy(_planes(filled, ld)).cuda()
@@ -49,7 +49,8 @@ def _noalloc_step(c, filled, ld, dt, out_fill=0.0):
     sc = to_c_control(c)
     cfl = C.c_double()
     ierr = C.c_int()
-    rc = L.pcl_solve_dimensional_split_noalloc(C.byref(sc), 0, None, C.c_void_p(d_in.data_ptr()),
+    handle = C.c_void_p(stream.cuda_stream) if stream is not None else None
+    rc = L.pcl_solve_dimensional_split_noalloc(C.byref(sc), 0, handle, C.c_void_p(d_in.data_ptr()),
                                                C.c_void_p(d_out.data_ptr()), ld, dt, C.byref(cfl), C.byref(ierr))
     torch.cuda.synchronize()
     out = d_out.cpu().numpy()
@@ -88,6 +89,21 @@ def test_noalloc_matches_regular_step_twice_in_a_row(pcl):
         results.append(out_n)
     # the repeated first case is unaffected by what the previous call left in the scratch
     assert np.array_equal(results[0], results[2])
+
+
+def test_noalloc_on_a_caller_stream_keeps_the_current_device(pcl):
+    """The stream argument: a caller's own (non-default) stream; the call leaves the caller's
+    current device as it found it."""
+    import torch
+    for case in (_case_b, _case_a):
+        c, q, ld = case()
+        filled, ierr, cfl, out = _regular_step(c, q)
+        before = torch.cuda.current_device()
+        st = torch.cuda.Stream()
+        rc, ierr_n, cfl_n, out_n, _ = _noalloc_step(c, filled, ld, c.initial_timestep, stream=st)
+        assert torch.cuda.current_device() == before
+        assert rc == 0 and ierr_n == ierr == 1 and cfl_n == cfl
+        assert np.array_equal(out_n, out)
 
 
 def test_noalloc_rejected_attempt_leaves_output(pcl):
