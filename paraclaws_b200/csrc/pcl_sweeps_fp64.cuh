@@ -229,7 +229,9 @@ __device__ __forceinline__ void y_corr_flux(const Waves& Wm, const Waves& W, con
   for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
 }
 
-template <int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
+// UNR unrolls the row loop (the window's shift then becomes register renaming); it changes no
+// arithmetic.
+template <int LIM, bool SO, int MK = kMetricTable, int OPT = 0, int UNR = 1>
 __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   Ctl* ctl = g.ctl;
@@ -304,6 +306,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
     s1 = iface(j0 + 1, cA, cB, W1);
     if constexpr (SO) y_corr_flux<LIM, SO, UM, OPT>(Wm, W0, W1, s0, true, dtod, cm1.kap, cA.kap, ft0);
   }
+#pragma unroll UNR
   for (int jj = j0; jj <= j1; ++jj) {
     load(jj + 2, cC);
     s2w = iface(jj + 2, cB, cC, W2);
