@@ -663,6 +663,11 @@ int pcl_get_stats(pcl_ctx* x, pcl_run_stats* s) {
 }
 
 static void enqueue_attempt(pcl_ctx* x) {
+  if (x->cfg.precision_mode == PCL_PREC_MIXED && !x->source && !x->user_bc && !mixed_injection_on(x->mixed)) {
+    launch_step_mixed(x->g, x->mixed, x->stream);  // sweeps, time control and ghost fill in one launch
+    x->launches += 1;
+    return;
+  }
   launch_sweeps(x);
   launch_timectl(x->g, kOpFullStep, 0, 0.0, x->stream);
   enqueue_source(x, 0);

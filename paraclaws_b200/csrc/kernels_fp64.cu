@@ -14,15 +14,21 @@ namespace pcl {
 // launchers
 // ------------------------------------------------------------------------------------------
 namespace {
-// Launch shapes (measured on B200, 4096^2 minmod): the xi sweep at 5 CTAs of 256 threads per SM
-// (48 registers) and the eta sweep at 6 CTAs of 128 threads per SM (80 registers, a few spilled
-// window values) with 16-row strips beat the unconstrained register counts (4 CTAs each) by
-// 20 %: both kernels are latency bound on chains of FP64 divisions and need the warps.
-constexpr int kXT = 256;   // threads (and slots) of an xi-sweep CTA
-constexpr int kXMinBlocks = 5;
+// Launch shapes (measured on B200, 4096^2 bumps after 300 steps, minmod; every variant
+// bit-identical): the xi sweep at 8 CTAs of 128 threads per SM, each CTA sweeping 8 rows of its
+// segment with one block reduction at the end, with the shared-reciprocal quotients
+// (kOptFastDiv): 0.391 ms against 0.508 ms for one row per 256-thread CTA at 5 CTAs per SM (4
+// rows: 0.397; the limiter shortcut on top: 0.399).  The eta sweep at 6 CTAs of 128 threads per
+// SM (80 registers, a few spilled window values) with 24-row strips: 0.487 ms (16 rows: 0.492,
+// 32: 0.492).  Neither shortcut nor unrolling its row loop helps it (more registers, more
+// spills), and the xi sweep's phases run along columns of transposed tiles (ysweep_tile) are
+// slower (0.516 ms at best, with 4-column tiles and four tiles per CTA).
+constexpr int kXT = 128;   // threads (and slots) of an xi-sweep CTA
+constexpr int kXMinBlocks = 8;
+constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA
 constexpr int kYT = 128;   // columns of an eta-sweep CTA
 constexpr int kYMinBlocks = 6;
-constexpr int kYS = 16;    // rows of an eta-sweep strip
+constexpr int kYS = 24;    // rows of an eta-sweep strip
 
 // A CTA sweeps R consecutive rows of one segment (blockIdx.y*R ..), strided by gridDim.y*R
 // when the grid has more rows than one launch's blocks cover.
@@ -48,10 +54,17 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
   ysweep_strip<LIM, SO, MK>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
 }
 
+// The shortcuts' range argument assumes g in [2^-20, 2^20] (pcl_fp64.cuh: kOptFastDiv).
+inline bool fast_div_ok(const GridDev& g) { return g.grav >= 0x1p-20 && g.grav <= 0x1p20; }
+
 template <int LIM, bool SO, int MK>
 void launch_x_t(const GridDev& g, cudaStream_t st) {
-  dim3 gx((g.mx + (kXT - 4) - 1) / (kXT - 4), g.my < 65535 ? g.my : 65535);
-  xsweep_fp64_kernel<kXT, LIM, SO, MK><<<gx, kXT, 0, st>>>(g);
+  const int rb = (g.my + kXRows - 1) / kXRows;
+  dim3 gx((g.mx + (kXT - 4) - 1) / (kXT - 4), rb < 65535 ? rb : 65535);
+  if (fast_div_ok(g))
+    xsweep_fp64_kernel<kXT, LIM, SO, MK, kXRows, kOptFastDiv><<<gx, kXT, 0, st>>>(g);
+  else
+    xsweep_fp64_kernel<kXT, LIM, SO, MK, kXRows><<<gx, kXT, 0, st>>>(g);
 }
 template <int LIM, bool SO, int MK>
 void launch_y_t(const GridDev& g, cudaStream_t st) {

@@ -3,8 +3,10 @@
 #include <cuda_runtime.h>
 
 #include "../../include/paraclaws_b200.h"
+#include "pcl_ghost.cuh"
 #include "pcl_mixed.h"
 #include "pcl_stream_mixed.cuh"
+#include "pcl_timectl.cuh"
 
 namespace pcl {
 namespace mixed {
@@ -19,6 +21,44 @@ __global__ void __launch_bounds__(NT) fused_mixed_kernel(GridDev g, int TY, int 
   init_ring(S);
   unsigned rows = 0;
   mixed_item<LIM, SO, 2, INJ>(g, blockIdx.x % nstrips, blockIdx.x / nstrips, TY, S, rows, inj_row, probes);
+}
+
+// The whole attempt in one launch (the device loop when no host hook runs between the time
+// control and the ghost fill): a CTA whose item lies on the edge of the grid fills the ghost
+// cells next to the cells it wrote, into the step's output buffer (unused if the step is
+// rejected); the CTA that finishes the last item runs the time control (full_step: CFL,
+// accept/reject, updateTime, snapshot index, reset_CFL, log) and, after an accepted step, the
+// ghost sides no item could fill (a last strip or segment one cell wide).  The same values as
+// the separate time-control and ghost kernels: only where they are computed changes.
+template <int LIM, bool SO>
+__global__ void __launch_bounds__(NT, 5) fused_mixed_step_kernel(GridDev g, int TY, int nstrips) {
+  __shared__ Smem S;
+  __shared__ int s_last;
+  Ctl* ctl = g.ctl;
+  if (ctl->done) return;
+  init_ring(S);
+  unsigned rows = 0;
+  const int strip = blockIdx.x % nstrips, seg = blockIdx.x / nstrips;
+  const bool ok = mixed_item<LIM, SO, 2>(g, strip, seg, TY, S, rows);
+  if (ok && (strip == 0 || seg == 0 || (strip + 1) * TXI >= g.mx || (seg + 1) * TY >= g.my)) {
+    const int cur = ctl->cur;
+    const int i0 = 1 + strip * TXI, j0 = 1 + seg * TY;
+    ghost_fill_block(g, buffer(g, cur == 0 ? 2 : cur - 1), i0, min(i0 + TXI - 1, g.mx), j0, min(j0 + TY - 1, g.my));
+  }
+  __threadfence();  // every thread's writes of this item precede its completion count
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_last = atomicAdd(&ctl->items_done, 1) + 1 == (int)gridDim.x;
+    if (s_last) {
+      __threadfence();
+      full_step(ctl, g);
+      ctl->items_done = 0;
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  if (s_last && ctl->ierr == 1)
+    ghost_fill_open_sides(g, buffer(g, ctl->cur), (g.mx - 1) % TXI == 0, (g.my - 1) % TY == 0);
 }
 
 struct Workspace {
@@ -74,6 +114,32 @@ void launch_t(const GridDev& g, const mixed::Workspace* w, cudaStream_t st) {
     mixed::fused_mixed_kernel<LIM, SO><<<nstrips * nseg, mixed::NT, 0, st>>>(g, ty, nstrips, -1, 0u);
 }
 }  // namespace
+
+namespace {
+template <int LIM, bool SO>
+void launch_step_t(const GridDev& g, const mixed::Workspace* w, cudaStream_t st) {
+  const int ty = w ? w->ty : 64;
+  const int nstrips = (g.mx + mixed::TXI - 1) / mixed::TXI;
+  const int nseg = (g.my + ty - 1) / ty;
+  mixed::fused_mixed_step_kernel<LIM, SO><<<nstrips * nseg, mixed::NT, 0, st>>>(g, ty, nstrips);
+}
+}  // namespace
+
+void launch_step_mixed(const GridDev& g, void* ws, cudaStream_t st) {
+  const auto* w = static_cast<const mixed::Workspace*>(ws);
+  if (!g.second_order) return launch_step_t<0, false>(g, w, st);
+  switch (g.limiter) {
+    case 1: return launch_step_t<1, true>(g, w, st);
+    case 2: return launch_step_t<2, true>(g, w, st);
+    case 3: return launch_step_t<3, true>(g, w, st);
+    case 4: return launch_step_t<4, true>(g, w, st);
+    default: return launch_step_t<0, true>(g, w, st);
+  }
+}
+
+bool mixed_injection_on(const void* ws) {
+  return ws && static_cast<const mixed::Workspace*>(ws)->inj_row >= 0;
+}
 
 void launch_sweeps_mixed(const GridDev& g, void* ws, cudaStream_t st) {
   const auto* w = static_cast<const mixed::Workspace*>(ws);

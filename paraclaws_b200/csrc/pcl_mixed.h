@@ -12,4 +12,8 @@ void mixed_set_tile_rows(void* ws, int ty);   // rows per work item of the fused
 // `probes` probes (row < 0: off)
 void mixed_set_injection(void* ws, int row, unsigned probes);
 void launch_sweeps_mixed(const GridDev& g, void* ws, cudaStream_t st);
+// one whole attempt of the device loop in one launch: the fused sweeps, then the time control
+// and the ghost fill by the CTAs (no host hook may run in between)
+void launch_step_mixed(const GridDev& g, void* ws, cudaStream_t st);
+bool mixed_injection_on(const void* ws);   // a copy stall is injected (the test build runs)
 }  // namespace pcl

@@ -67,6 +67,8 @@ struct Ctl {
   unsigned long long smax_x, smax_y;  // IEEE bits of max wave speed s2 per sweep (>= 0)
   double cfl_x, cfl_y;       // CFL_local after the xi sweep / after both sweeps
   int valid_x;               // xi-sweep validity (early reject, MOD_solve.f90:107-120)
+  int items_done;            // work items of the attempt finished so far (kernels whose last CTA
+                             // runs the time control); the last one resets it
   int ierr;                  // last attempt: 1 accepted, -1 rejected, 0 none yet
   int cur;                   // index of the current state buffer (0..2)
   int done;                  // time >= time_final, accepted-step cap reached, or error

@@ -121,3 +121,35 @@ def test_mixed_reports_bad_state(pcl):
     with pytest.raises(PclError) as e:
         s.advance()
     assert e.value.code == PCL_ERR_NAN
+
+
+@pytest.mark.parametrize("mx,my,lim,bc,tile", [
+    (125, 129, 1, 1, 64),     # last strip and last row segment one cell wide: the finisher's sides
+    (260, 97, 4, 3, 32),
+    (64, 40, 2, 2, 16),
+])
+def test_single_launch_device_loop_equals_host_driven_steps(pcl, mx, my, lim, bc, tile):
+    """The device loop runs each mixed attempt as one launch (edge CTAs fill their ghost cells,
+    the last CTA runs the time control and the remaining ghost sides); the host-driven loop runs
+    the sweeps, the time control and the ghost fill as separate kernels.  Same bits, same dt
+    sequence."""
+    from paraclaws_b200.solver import run_host_loop
+    c = dataclasses.replace(ctl.dam_break_control(mx, limiter=lim, bc=bc, time_final=100.0), m_eta=my)
+    cu = ctl.CustomSettings(max_accepted_steps=40)
+    q = ic.gaussian_bumps(mx, my, seed=6)
+    out = []
+    for device_loop in (True, False):
+        s = Solver(c, cu, precision=ctl.PRECISION_MIXED)
+        s.set_tile_rows(tile)
+        s.upload(q)
+        s.update_rank_boundaries()
+        if device_loop:
+            s.advance()
+            lg = s.step_log()
+        else:
+            lg = run_host_loop(s)
+        out.append((s.download(), lg.dt, lg.ierr))
+        s.close()
+    assert len(out[0][1]) == len(out[1][1]) > 30
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][0].view(np.int64), out[1][0].view(np.int64))

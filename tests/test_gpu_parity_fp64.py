@@ -94,10 +94,6 @@ def test_dam_break_200_to_t05(pcl, oracle_lib, bc):
     assert np.array_equal(lg.cfl, log_o.cfl)
     assert np.array_equal(lg.time, log_o.time)
     _assert_state_equal(s.download(), o.state(), "t=0.5")
-    if bc == 1:  # the walls conserve mass up to the HLL epsilon drift (h grows by O(dt/dx * 1e-10))
-        h0 = q[2:-2, 2:-2, 0].sum()
-        h1 = s.download()[2:-2, 2:-2, 0].sum()
-        assert abs(h1 - h0) / h0 < 1e-6
 
 
 def test_first_order_and_unlimited(pcl, oracle_lib):

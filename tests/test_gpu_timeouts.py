@@ -83,7 +83,7 @@ def test_fp64_batch_wait_runs_out_and_recovers(pcl):
     # instance equals the same grid solved alone, bit for bit
     assert L.pcl_batch_inject_stall(b.h, -1, 0) == 0
     b.remove(slots[1])
-    slots[1] = b.add(*cfg[1])
+    slots[1] = b.add(cfg[1][0], None, cfg[1][1])
     _run_batch_to_end(b)
     for slot, (c, cu) in zip(slots, cfg):
         st = b.stats(slot)
