@@ -342,11 +342,7 @@ int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
   const int pitch = (ni + 31) / 32 * 32;
   const long long plane = (long long)pitch * nj;
   const int neq = c->num_equations;
-  // the FP64 sweeps' intermediate may be held transposed: room for either layout
-  const int tpitch = (nj + 31) / 32 * 32;
-  const long long tplane = (long long)tpitch * ni;
-  const long long plane_room = plane > tplane ? plane : tplane;
-  const size_t buf_bytes = sizeof(double) * 3 * (size_t)neq * (size_t)plane_room;
+  const size_t buf_bytes = sizeof(double) * 3 * (size_t)neq * (size_t)plane;
   const double dxi = (c->xi_max - c->xi_min) / c->m_xi;     // :28
   const double deta = (c->eta_max - c->eta_min) / c->m_eta;  // :29
   std::vector<double> rowm, colm;
@@ -374,9 +370,7 @@ int pcl_create(const pcl_solver_control* c, int device, pcl_ctx** out) {
     return fail(PCL_ERR_CUDA);
   GridDev& g = x->g;
   g.state = x->bufs_d;
-  g.bufstride = (long long)neq * plane_room;
-  g.tpitch = neq == 3 ? tpitch : 0;
-  g.tplane = tplane;
+  g.bufstride = (long long)neq * plane;
   g.neq = neq;
   g.eq = neq == 3 ? PCL_EQ_SHALLOW_WATER : -1;  // other sizes need a module (pcl_set_equation)
   g.rowm = x->tables_d;

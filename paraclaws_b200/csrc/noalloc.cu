@@ -169,9 +169,7 @@ extern "C" int pcl_solve_dimensional_split_noalloc(const pcl_solver_control* c, 
   h.log = nullptr;
 
   g.state = base;
-  g.tpitch = (my + 4 + 31) / 32 * 32;  // the transposed intermediate fits the same room
-  g.tplane = (long long)g.tpitch * (mx + 4);
-  g.bufstride = 3 * (plane > g.tplane ? plane : g.tplane);
+  g.bufstride = 3 * plane;
   g.neq = 3;
   g.rowm = base + kTableOffset;
   g.colm = base + kTableOffset + (long long)(my + 4) * pcl::kRowMetrics;

@@ -355,15 +355,24 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
 }
 
 // ------------------------------------------------------------------------------------------
-// The sweeps through a transposed intermediate (uniform grids).  Both directions run the xi
-// sweep's four shared-memory phases on one line of cells: line_sweep.  The xi sweep writes its
-// result transposed, so the eta sweep reads its lines (columns of the grid) as contiguous
-// memory, and writes its result back in the normal layout.  A thread keeps its cell's result
-// of two consecutive lines and writes them as one 16-byte pair: the transposes move whole
-// sectors.  Same semantics as xsweep_segment and ysweep_strip: the eta sweep's ghost rows come
-// from the pre-step buffer (P11), the last interface is unlimited, the pre-step ghost cells are
-// carried into the new buffer.
+// eta sweep in phases.  The xi sweep's four shared-memory phases run along the columns of a tile
+// of TX columns x L rows: slot t = r*TX + c holds cell (i0 + c, j0 - 2 + r), so a warp's loads
+// and stores are TX*8 contiguous bytes on each of 32/TX rows, and the neighbour of a slot along
+// the column is t +- TX.  A tile updates rows j0 .. j0+L-5 of its columns; tile columns start at
+// i = -1 + TX*k, so their rows start on 32-byte sector boundaries (columns outside 1 .. m_xi are
+// computed on a clamped column and written nowhere).  Same semantics as ysweep_strip: rows
+// 1 .. m_eta come from the xi-swept buffer and the ghost rows from the pre-step buffer (P11),
+// getJakobi's status counts rows -1 .. m_eta+1, the last interface (m_eta+1) is unlimited, the
+// pre-step ghost cells are carried into the new buffer.  The caller checks the xi-sweep validity
+// (eta_valid) and reduces the wave-speed maximum over the CTA (eta_finish).
 // ------------------------------------------------------------------------------------------
+template <int NT>
+struct YSmem {
+  double sq[3][NT], sf[3][NT], ss[NT], sk[NT], slr[NT];
+  double sw1[3][NT], sw2[3][NT], ss2[NT], sft[3][NT];
+  double red[NT / 32];
+  bool sok[NT];
+};
 
 // xi-sweep validity (MOD_solve.f90:107-120) from the reduction word of the xi sweep
 __device__ __forceinline__ bool eta_valid(const GridDev& g) {
@@ -374,62 +383,71 @@ __device__ __forceinline__ bool eta_valid(const GridDev& g) {
   return ctl->CFL_target / cfl >= ctl->shrink;
 }
 
-// One line of the sweep in direction DIR: DIR 0 the row j = line of buffer cur (normal layout),
-// DIR 1 the column i = line of the transposed xi-swept buffer, with its ghost rows from buffer
-// cur.  Cells i0-2+t are loaded, cells i0+t (t < NT-4) updated: returns true and the new values
-// in out[] for a thread whose cell lies inside the line.  All threads of the CTA call it.
-template <int NT, int DIR, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
-__device__ __forceinline__ bool line_sweep(const GridDev& g, int line, int i0, XSmem<NT>& S, double& smax_acc,
-                                           int& bad_acc, double out[3]) {
-  constexpr bool UM = MK == kMetricUnit;
+template <int NT>
+__device__ __forceinline__ void eta_finish(const GridDev& g, double smax, int bad, YSmem<NT>& S) {
+  block_max_to<NT>(&g.ctl->smax_y, smax, S.red);
+  if (bad) atomicOr(&g.ctl->status, bad);
+}
+
+template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
+__device__ __forceinline__ void ysweep_tile(const GridDev& g, int i0, int j0, YSmem<NT>& S, double& smax_acc,
+                                            int& bad_acc) {
+  constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
+  constexpr int L = NT / TX;
   const Ctl* ctl = g.ctl;
-  constexpr int L = NT - 4;
-  const int cur = ctl->cur, xb = cur == 2 ? 0 : cur + 1;
-  const double dtod = DIR == 0 ? ctl->dtod_x : ctl->dtod_y;
+  const int cur = ctl->cur;
+  const int xb = cur == 2 ? 0 : cur + 1;
+  const int yb = cur == 0 ? 2 : cur - 1;
+  const double dtod = ctl->dtod_y;
+  const int mx = g.mx, my = g.my;
+  const long long P = g.pitch;
   const int t = threadIdx.x;
-  const int mlen = DIR == 0 ? g.mx : g.my;  // cells along the line
+  const int cx = t % TX, r = t / TX;
+  const int i = i0 + cx;
+  const bool active = i >= 1 && i <= mx;
+  const int ic = i < 1 ? 1 : (i > mx ? mx : i);  // inactive columns shadow a valid one
   const double* pre = buffer(g, cur);
+  const double* xsw = buffer(g, xb);
+  double* outp = buffer(g, yb);
 
   int bad = 0;
-  {  // phase A: per-cell flux, wave-speed bound and capacity of cell c = i0-2+t
-    const int c = i0 - 2 + t;
-    if (c <= mlen + 2) {
-      const double* q;
-      long long ps;
-      if (DIR == 0) {
-        q = pre + (long long)(line + 1) * g.pitch + (c + 1), ps = g.plane;
-      } else if (c >= 1 && c <= mlen) {
-        q = buffer(g, xb) + (long long)(line + 1) * g.tpitch + (c + 1), ps = g.tplane;
-      } else {  // a ghost row: the pre-step fill (P11)
-        q = pre + (long long)(c + 1) * g.pitch + (line + 1), ps = g.plane;
-      }
-      const double h = q[0], hu = q[ps], hv = q[2 * ps];
+  {  // phase A: cell j = j0-2+r of column ic
+    const int j = j0 - 2 + r;
+    if (j <= my + 2) {
+      const double* src = (j >= 1 && j <= my) ? xsw : pre;
+      const long long o = (long long)(j + 1) * P + (ic + 1);
+      const double h = src[o], hu = src[o + g.plane], hv = src[o + 2 * g.plane];
       int cb = 0;
-      const CellFlux F = cell_flux<DIR, OPT>(h, hu, hv, g.grav, &cb);
-      if (c <= mlen + 1) bad |= cb;  // getJakobi runs on cells -1 .. m+1 along the line
+      const CellFlux F = cell_flux<1, OPT>(h, hu, hv, g.grav, &cb);
+      if (j <= my + 1 && active) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
       S.sq[0][t] = h; S.sq[1][t] = hu; S.sq[2][t] = hv;
       S.sf[0][t] = F.f0; S.sf[1][t] = F.f1; S.sf[2][t] = F.f2;
       S.ss[t] = F.s;
       if constexpr ((OPT & kOptFastDiv) != 0) S.sok[t] = F.ok;
-      if constexpr (!UM) S.sk[t] = DIR == 0 ? capacity(g.rowm, g.colm, c, line, g.area_scale)
-                                             : capacity(g.rowm, g.colm, line, c, g.area_scale);
+      if constexpr (MP) {
+        S.sk[t] = __ldg(g.kap + o);
+        S.slr[t] = __ldg(g.lry + o);
+      } else if constexpr (!UM) {
+        S.sk[t] = capacity(g.rowm, g.colm, ic, j, g.area_scale);
+      }
     }
   }
   __syncthreads();
 
   double smax = 0.0;
-  if (t < NT - 1) {  // phase B: HLL at interface k = i0-1+t between slots t and t+1
-    const int k = i0 - 1 + t;
+  if (r < L - 1) {  // phase B: HLL at interface k = j0-1+r between slots t and t+TX
+    const int k = j0 - 1 + r;
     Waves W;
     double s2 = 0.0;
-    if (k <= mlen + 1) {
+    if (k <= my + 1) {
+      const int u = t + TX;
       const double qL[3] = {S.sq[0][t], S.sq[1][t], S.sq[2][t]};
-      const double qR[3] = {S.sq[0][t + 1], S.sq[1][t + 1], S.sq[2][t + 1]};
+      const double qR[3] = {S.sq[0][u], S.sq[1][u], S.sq[2][u]};
       CellFlux FL = {S.sf[0][t], S.sf[1][t], S.sf[2][t], S.ss[t]};
-      CellFlux FR = {S.sf[0][t + 1], S.sf[1][t + 1], S.sf[2][t + 1], S.ss[t + 1]};
-      if constexpr ((OPT & kOptFastDiv) != 0) FL.ok = S.sok[t], FR.ok = S.sok[t + 1];
+      CellFlux FR = {S.sf[0][u], S.sf[1][u], S.sf[2][u], S.ss[u]};
+      if constexpr ((OPT & kOptFastDiv) != 0) FL.ok = S.sok[t], FR.ok = S.sok[u];
       s2 = hll<OPT>(qL, FL, qR, FR, W);
-      smax = s2;
+      if (active) smax = s2;
     } else {
 #pragma unroll
       for (int me = 0; me < 3; ++me) W.w1[me] = W.w2[me] = 0.0;
@@ -445,23 +463,23 @@ __device__ __forceinline__ bool line_sweep(const GridDev& g, int line, int i0, X
   bad_acc |= bad;
   __syncthreads();
 
-  if constexpr (SO) {  // phase C: correction flux at interface k = i0+t (slot t+1)
-    if (t < NT - 3) {
-      const int k = i0 + t;
+  if constexpr (SO) {  // phase C: correction flux at interface k = j0+r (slot t+TX)
+    if (r < L - 3) {
+      const int k = j0 + r;
       double ft[3] = {0.0, 0.0, 0.0};
-      if (k <= mlen + 1) {
-        const int s = t + 1;
+      if (k <= my + 1) {
+        const int s = t + TX;
         const double s2 = S.ss2[s];
-        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, S.sk[t + 1], S.sk[t + 2]);
+        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, S.sk[t + TX], S.sk[t + 2 * TX]);
         if (cf != 0.0) {
           const double w1[3] = {S.sw1[0][s], S.sw1[1][s], S.sw1[2][s]};
           const double w2[3] = {S.sw2[0][s], S.sw2[1][s], S.sw2[2][s]};
           double a[3], b[3];
-          if (LIM != 0 && k <= mlen) {  // the last interface (m+1) stays unlimited
-            const double w1m[3] = {S.sw1[0][s - 1], S.sw1[1][s - 1], S.sw1[2][s - 1]};
-            const double w1p[3] = {S.sw1[0][s + 1], S.sw1[1][s + 1], S.sw1[2][s + 1]};
-            const double w2m[3] = {S.sw2[0][s - 1], S.sw2[1][s - 1], S.sw2[2][s - 1]};
-            const double w2p[3] = {S.sw2[0][s + 1], S.sw2[1][s + 1], S.sw2[2][s + 1]};
+          if (LIM != 0 && k <= my) {
+            const double w1m[3] = {S.sw1[0][s - TX], S.sw1[1][s - TX], S.sw1[2][s - TX]};
+            const double w1p[3] = {S.sw1[0][s + TX], S.sw1[1][s + TX], S.sw1[2][s + TX]};
+            const double w2m[3] = {S.sw2[0][s - TX], S.sw2[1][s - TX], S.sw2[2][s - TX]};
+            const double w2p[3] = {S.sw2[0][s + TX], S.sw2[1][s + TX], S.sw2[2][s + TX]};
             limit_wave<LIM, OPT>(w1m, w1, w1p, false, a);  // lambda_1 = -s2 <= 0
             limit_wave<LIM, OPT>(w2m, w2, w2p, s2 > 0.0, b);
           } else {
@@ -481,34 +499,52 @@ __device__ __forceinline__ bool line_sweep(const GridDev& g, int line, int i0, X
     __syncthreads();
   }
 
-  // phase D: the new value of cell i0+t (MOD_solve.f90:207-221 and :268-278)
-  if (t >= L || i0 + t > mlen) return false;
-  const int c = t + 2;
-  const double gam = UM ? 1.0 : (DIR == 0 ? __ldg(g.rowm + (line + 1) * kRowMetrics + 2)
-                                          : __ldg(g.colm + (line + 1) * kColMetrics + 2));
-  const double dtk = UM ? dtod : dtod / S.sk[c];
-  const double sp = S.ss2[t + 1];   // A+ at interface i0+t:   s2 * W2
-  const double sm = -S.ss2[t + 2];  // A- at interface i0+t+1: s1 * W1
+  // phase D: update of cell j = j0+r (slot t+2TX)
+  const int jl = min(j0 + L - 5, my);
+  if (r < L - 4 && active) {
+    const int j = j0 + r;
+    if (j <= my) {
+      const int c = t + 2 * TX;
+      const double gam = (UM || MP) ? 1.0 : __ldg(g.colm + (ic + 1) * kColMetrics + 2);
+      const double gl = MP ? S.slr[c] : gam;       // face between rows j-1 and j
+      const double gr = MP ? S.slr[c + TX] : gam;  // face between rows j and j+1
+      const double dtk = UM ? dtod : dtod / S.sk[c];
+      const double sp = S.ss2[t + TX];         // A+ at interface j:   s2 * W2
+      const double sm = -S.ss2[t + 2 * TX];    // A- at interface j+1: s1 * W1
+      const long long o = (long long)(j + 1) * P + (i + 1);
 #pragma unroll
-  for (int me = 0; me < 3; ++me) {
-    const double ap = sp * S.sw2[me][t + 1];
-    const double am = sm * S.sw1[me][t + 2];
-    double q = UM ? S.sq[me][c] - dtk * (ap + am) : S.sq[me][c] - dtk * (gam * ap + gam * am);
-    if constexpr (SO) q = q - dtk * (S.sft[me][t + 1] - S.sft[me][t]);
-    out[me] = q;
+      for (int me = 0; me < 3; ++me) {
+        const double ap = sp * S.sw2[me][t + TX];
+        const double am = sm * S.sw1[me][t + 2 * TX];
+        double q = UM ? S.sq[me][c] - dtk * (ap + am) : S.sq[me][c] - dtk * (gl * ap + gr * am);
+        if constexpr (SO) q = q - dtk * (S.sft[me][t + TX] - S.sft[me][t]);
+        outp[o + me * g.plane] = q;
+      }
+    }
   }
-  return true;
-}
-
-// Store one cell's three values (plane stride ps) at dst, or a pair of cells (dst, dst+1) from
-// two consecutive lines as 16-byte stores; dst of a pair is 16-byte aligned.
-__device__ __forceinline__ void store_cell(double* dst, long long ps, const double v[3]) {
+  // the pre-step ghost cells carried into the new buffer (main.f90:210 vs :246): the ghost rows
+  // of the tile's columns when the tile starts at row 1 or ends at row m_eta, and the ghost
+  // columns next to columns 1 and m_xi over the tile's rows
+  if (active && r < 4) {
+    auto copy_cell = [&](int ci, int cj) {
+      const long long o = (long long)(cj + 1) * P + (ci + 1);
 #pragma unroll
-  for (int me = 0; me < 3; ++me) dst[me * ps] = v[me];
-}
-__device__ __forceinline__ void store_pair(double* dst, long long ps, const double a[3], const double b[3]) {
+      for (int me = 0; me < 3; ++me) outp[o + me * g.plane] = pre[o + me * g.plane];
+    };
+    if (r < 2 && j0 == 1) copy_cell(i, -1 + r);
+    if (r >= 2 && jl == my) copy_cell(i, my + r - 1);
+  }
+  if (active && (i == 1 || i == mx) && r < L - 4) {
+    const int j = j0 + r;
+    if (j <= my) {
+      const long long o = (long long)(j + 1) * P;
+      const int g0 = i == 1 ? -1 : mx + 1;
 #pragma unroll
-  for (int me = 0; me < 3; ++me) *reinterpret_cast<double2*>(dst + me * ps) = make_double2(a[me], b[me]);
+      for (int gcol = g0; gcol <= g0 + 1; ++gcol)
+#pragma unroll
+        for (int me = 0; me < 3; ++me) outp[o + gcol + 1 + me * g.plane] = pre[o + gcol + 1 + me * g.plane];
+    }
+  }
 }
 
 }  // namespace pcl

@@ -91,10 +91,6 @@ struct GridDev {
   Ctl* ctl;
   long long plane;           // doubles per plane
   int mx, my, pitch;
-  // the transposed layout of the FP64 sweeps' intermediate (xi-swept) state: cell (i, j) of
-  // plane p at p*tplane + (i+1)*tpitch + (j+1); tpitch a multiple of 32 (0: not used)
-  int tpitch;
-  long long tplane;
   int bc[4];                 // xi_low, xi_high, eta_low, eta_high (1 wall, 2 zero grad., 3 const. grad.)
   int second_order, limiter; // limiter 0: unlimited correction; 1..4 by code
   int metric;                // kMetric*
