@@ -20,9 +20,11 @@ namespace {
 // (kOptFastDiv): 0.391 ms against 0.508 ms for one row per 256-thread CTA at 5 CTAs per SM (4
 // rows: 0.397; the limiter shortcut on top: 0.399).  The eta sweep at 6 CTAs of 128 threads per
 // SM (80 registers, a few spilled window values) with 24-row strips: 0.487 ms (16 rows: 0.492,
-// 32: 0.492).  Neither shortcut nor unrolling its row loop helps it (more registers, more
-// spills), and the xi sweep's phases run along columns of transposed tiles (ysweep_tile) are
-// slower (0.516 ms at best, with 4-column tiles and four tiles per CTA).
+// 32: 0.492).  Measured and dropped for the eta sweep: the two shortcuts and an unrolled row
+// loop (more registers, more spills); the xi sweep's shared-memory phases run along the columns
+// of 4-column tiles (0.516 ms at best); and an xi sweep that stores its result transposed so the
+// eta sweep can read contiguous lines (0.645 + 0.653 ms: the strided stores cost more than the
+// phases save).
 constexpr int kXT = 128;   // threads (and slots) of an xi-sweep CTA
 constexpr int kXMinBlocks = 8;
 constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA

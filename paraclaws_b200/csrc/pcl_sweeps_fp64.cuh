@@ -354,197 +354,4 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
   if (bad) atomicOr(&ctl->status, bad);
 }
 
-// ------------------------------------------------------------------------------------------
-// eta sweep in phases.  The xi sweep's four shared-memory phases run along the columns of a tile
-// of TX columns x L rows: slot t = r*TX + c holds cell (i0 + c, j0 - 2 + r), so a warp's loads
-// and stores are TX*8 contiguous bytes on each of 32/TX rows, and the neighbour of a slot along
-// the column is t +- TX.  A tile updates rows j0 .. j0+L-5 of its columns; tile columns start at
-// i = -1 + TX*k, so their rows start on 32-byte sector boundaries (columns outside 1 .. m_xi are
-// computed on a clamped column and written nowhere).  Same semantics as ysweep_strip: rows
-// 1 .. m_eta come from the xi-swept buffer and the ghost rows from the pre-step buffer (P11),
-// getJakobi's status counts rows -1 .. m_eta+1, the last interface (m_eta+1) is unlimited, the
-// pre-step ghost cells are carried into the new buffer.  The caller checks the xi-sweep validity
-// (eta_valid) and reduces the wave-speed maximum over the CTA (eta_finish).
-// ------------------------------------------------------------------------------------------
-template <int NT>
-struct YSmem {
-  double sq[3][NT], sf[3][NT], ss[NT], sk[NT], slr[NT];
-  double sw1[3][NT], sw2[3][NT], ss2[NT], sft[3][NT];
-  double red[NT / 32];
-  bool sok[NT];
-};
-
-// xi-sweep validity (MOD_solve.f90:107-120) from the reduction word of the xi sweep
-__device__ __forceinline__ bool eta_valid(const GridDev& g) {
-  const Ctl* ctl = g.ctl;
-  const double sx = __longlong_as_double((long long)__ldcg(&ctl->smax_x));
-  const double cflx = sx * ctl->dt / g.dxi;
-  const double cfl = fmax(ctl->CFL, cflx);
-  return ctl->CFL_target / cfl >= ctl->shrink;
-}
-
-template <int NT>
-__device__ __forceinline__ void eta_finish(const GridDev& g, double smax, int bad, YSmem<NT>& S) {
-  block_max_to<NT>(&g.ctl->smax_y, smax, S.red);
-  if (bad) atomicOr(&g.ctl->status, bad);
-}
-
-template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
-__device__ __forceinline__ void ysweep_tile(const GridDev& g, int i0, int j0, YSmem<NT>& S, double& smax_acc,
-                                            int& bad_acc) {
-  constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
-  constexpr int L = NT / TX;
-  const Ctl* ctl = g.ctl;
-  const int cur = ctl->cur;
-  const int xb = cur == 2 ? 0 : cur + 1;
-  const int yb = cur == 0 ? 2 : cur - 1;
-  const double dtod = ctl->dtod_y;
-  const int mx = g.mx, my = g.my;
-  const long long P = g.pitch;
-  const int t = threadIdx.x;
-  const int cx = t % TX, r = t / TX;
-  const int i = i0 + cx;
-  const bool active = i >= 1 && i <= mx;
-  const int ic = i < 1 ? 1 : (i > mx ? mx : i);  // inactive columns shadow a valid one
-  const double* pre = buffer(g, cur);
-  const double* xsw = buffer(g, xb);
-  double* outp = buffer(g, yb);
-
-  int bad = 0;
-  {  // phase A: cell j = j0-2+r of column ic
-    const int j = j0 - 2 + r;
-    if (j <= my + 2) {
-      const double* src = (j >= 1 && j <= my) ? xsw : pre;
-      const long long o = (long long)(j + 1) * P + (ic + 1);
-      const double h = src[o], hu = src[o + g.plane], hv = src[o + 2 * g.plane];
-      int cb = 0;
-      const CellFlux F = cell_flux<1, OPT>(h, hu, hv, g.grav, &cb);
-      if (j <= my + 1 && active) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1 in the eta sweep
-      S.sq[0][t] = h; S.sq[1][t] = hu; S.sq[2][t] = hv;
-      S.sf[0][t] = F.f0; S.sf[1][t] = F.f1; S.sf[2][t] = F.f2;
-      S.ss[t] = F.s;
-      if constexpr ((OPT & kOptFastDiv) != 0) S.sok[t] = F.ok;
-      if constexpr (MP) {
-        S.sk[t] = __ldg(g.kap + o);
-        S.slr[t] = __ldg(g.lry + o);
-      } else if constexpr (!UM) {
-        S.sk[t] = capacity(g.rowm, g.colm, ic, j, g.area_scale);
-      }
-    }
-  }
-  __syncthreads();
-
-  double smax = 0.0;
-  if (r < L - 1) {  // phase B: HLL at interface k = j0-1+r between slots t and t+TX
-    const int k = j0 - 1 + r;
-    Waves W;
-    double s2 = 0.0;
-    if (k <= my + 1) {
-      const int u = t + TX;
-      const double qL[3] = {S.sq[0][t], S.sq[1][t], S.sq[2][t]};
-      const double qR[3] = {S.sq[0][u], S.sq[1][u], S.sq[2][u]};
-      CellFlux FL = {S.sf[0][t], S.sf[1][t], S.sf[2][t], S.ss[t]};
-      CellFlux FR = {S.sf[0][u], S.sf[1][u], S.sf[2][u], S.ss[u]};
-      if constexpr ((OPT & kOptFastDiv) != 0) FL.ok = S.sok[t], FR.ok = S.sok[u];
-      s2 = hll<OPT>(qL, FL, qR, FR, W);
-      if (active) smax = s2;
-    } else {
-#pragma unroll
-      for (int me = 0; me < 3; ++me) W.w1[me] = W.w2[me] = 0.0;
-    }
-#pragma unroll
-    for (int me = 0; me < 3; ++me) {
-      S.sw1[me][t] = W.w1[me];
-      S.sw2[me][t] = W.w2[me];
-    }
-    S.ss2[t] = s2;
-  }
-  smax_acc = fmax(smax_acc, smax);
-  bad_acc |= bad;
-  __syncthreads();
-
-  if constexpr (SO) {  // phase C: correction flux at interface k = j0+r (slot t+TX)
-    if (r < L - 3) {
-      const int k = j0 + r;
-      double ft[3] = {0.0, 0.0, 0.0};
-      if (k <= my + 1) {
-        const int s = t + TX;
-        const double s2 = S.ss2[s];
-        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, S.sk[t + TX], S.sk[t + 2 * TX]);
-        if (cf != 0.0) {
-          const double w1[3] = {S.sw1[0][s], S.sw1[1][s], S.sw1[2][s]};
-          const double w2[3] = {S.sw2[0][s], S.sw2[1][s], S.sw2[2][s]};
-          double a[3], b[3];
-          if (LIM != 0 && k <= my) {
-            const double w1m[3] = {S.sw1[0][s - TX], S.sw1[1][s - TX], S.sw1[2][s - TX]};
-            const double w1p[3] = {S.sw1[0][s + TX], S.sw1[1][s + TX], S.sw1[2][s + TX]};
-            const double w2m[3] = {S.sw2[0][s - TX], S.sw2[1][s - TX], S.sw2[2][s - TX]};
-            const double w2p[3] = {S.sw2[0][s + TX], S.sw2[1][s + TX], S.sw2[2][s + TX]};
-            limit_wave<LIM, OPT>(w1m, w1, w1p, false, a);  // lambda_1 = -s2 <= 0
-            limit_wave<LIM, OPT>(w2m, w2, w2p, s2 > 0.0, b);
-          } else {
-#pragma unroll
-            for (int me = 0; me < 3; ++me) {
-              a[me] = w1[me];
-              b[me] = w2[me];
-            }
-          }
-#pragma unroll
-          for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
-        }
-      }
-#pragma unroll
-      for (int me = 0; me < 3; ++me) S.sft[me][t] = ft[me];
-    }
-    __syncthreads();
-  }
-
-  // phase D: update of cell j = j0+r (slot t+2TX)
-  const int jl = min(j0 + L - 5, my);
-  if (r < L - 4 && active) {
-    const int j = j0 + r;
-    if (j <= my) {
-      const int c = t + 2 * TX;
-      const double gam = (UM || MP) ? 1.0 : __ldg(g.colm + (ic + 1) * kColMetrics + 2);
-      const double gl = MP ? S.slr[c] : gam;       // face between rows j-1 and j
-      const double gr = MP ? S.slr[c + TX] : gam;  // face between rows j and j+1
-      const double dtk = UM ? dtod : dtod / S.sk[c];
-      const double sp = S.ss2[t + TX];         // A+ at interface j:   s2 * W2
-      const double sm = -S.ss2[t + 2 * TX];    // A- at interface j+1: s1 * W1
-      const long long o = (long long)(j + 1) * P + (i + 1);
-#pragma unroll
-      for (int me = 0; me < 3; ++me) {
-        const double ap = sp * S.sw2[me][t + TX];
-        const double am = sm * S.sw1[me][t + 2 * TX];
-        double q = UM ? S.sq[me][c] - dtk * (ap + am) : S.sq[me][c] - dtk * (gl * ap + gr * am);
-        if constexpr (SO) q = q - dtk * (S.sft[me][t + TX] - S.sft[me][t]);
-        outp[o + me * g.plane] = q;
-      }
-    }
-  }
-  // the pre-step ghost cells carried into the new buffer (main.f90:210 vs :246): the ghost rows
-  // of the tile's columns when the tile starts at row 1 or ends at row m_eta, and the ghost
-  // columns next to columns 1 and m_xi over the tile's rows
-  if (active && r < 4) {
-    auto copy_cell = [&](int ci, int cj) {
-      const long long o = (long long)(cj + 1) * P + (ci + 1);
-#pragma unroll
-      for (int me = 0; me < 3; ++me) outp[o + me * g.plane] = pre[o + me * g.plane];
-    };
-    if (r < 2 && j0 == 1) copy_cell(i, -1 + r);
-    if (r >= 2 && jl == my) copy_cell(i, my + r - 1);
-  }
-  if (active && (i == 1 || i == mx) && r < L - 4) {
-    const int j = j0 + r;
-    if (j <= my) {
-      const long long o = (long long)(j + 1) * P;
-      const int g0 = i == 1 ? -1 : mx + 1;
-#pragma unroll
-      for (int gcol = g0; gcol <= g0 + 1; ++gcol)
-#pragma unroll
-        for (int me = 0; me < 3; ++me) outp[o + gcol + 1 + me * g.plane] = pre[o + gcol + 1 + me * g.plane];
-    }
-  }
-}
-
 }  // namespace pcl
