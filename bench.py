@@ -564,11 +564,18 @@ def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), 
             l1_floor.append(float(np.abs(fb.download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
         fb.close()
         worst = int(np.argmax(l1_mixed))
+        worst_floor = int(np.argmax(l1_floor))
         res["l1_h_mixed_vs_fp64"] = {"median": float(np.median(l1_mixed)), "p99": float(np.percentile(l1_mixed, 99)),
-                                     "max": float(max(l1_mixed)), "max_instance_side": int(sides[worst]),
+                                     "max": float(max(l1_mixed)), "max_instance": worst,
+                                     "max_instance_side": int(sides[worst]),
+                                     "instances_le_1e-5": int(sum(v <= 1e-5 for v in l1_mixed)),
                                      "instances": n, "accepted_steps": accepted_steps}
         res["l1_h_fp64_floor"] = {"median": float(np.median(l1_floor)), "max": float(max(l1_floor)),
-                                  "note": "FP64 vs FP64 from the same start with h + 1 ulp in 1% of the cells"}
+                                  "max_instance": worst_floor, "of_mixed_max_instance": float(l1_floor[worst]),
+                                  "note": "FP64 vs FP64 from the same start with h + 1 ulp in 1% of the cells; "
+                                          "of_mixed_max_instance: the floor of the instance where mixed is "
+                                          "furthest from FP64 (an instance that amplifies any perturbation "
+                                          "shows it in both)"}
     for b in finals.values():
         b.close()
     res["instances"] = n
@@ -659,6 +666,8 @@ def target_summary(fp64_value: float, forms: dict) -> dict:
          "dram_roofline_frac": _sig(mx.get("dram_roofline_frac")),
          "l1_h_mixed_vs_fp64_median": _sig(l1.get("median")), "l1_h_mixed_vs_fp64_max": _sig(l1.get("max")),
          "l1_h_fp64_floor_median": _sig(fl.get("median")),
+         "l1_h_le_1e-5_instances": l1.get("instances_le_1e-5"),
+         "l1_h_fp64_floor_of_max_instance": _sig(fl.get("of_mixed_max_instance")),
          "serving_mixed": serve("mixed", 12.0), "serving_fp64": serve("fp64", 3.0),
          "workload": "C4, 512 instances x 200 accepted steps; serving C5"}
     if v:

@@ -193,6 +193,15 @@ int pcl_set_source_hook(pcl_ctx* ctx, pcl_source_fn fn, void* user);
 #define PCL_EQ_ACOUSTICS 2
 int pcl_set_equation(pcl_ctx* ctx, int module, const double* params, int nparams);
 
+/* Shape of the FP64 eta sweep, a schedule that never changes results.  PCL_SHAPE_AUTO (the
+   default) picks column windows when they fill the GPU with several waves of CTAs (large grids)
+   and 4-column bands below that; PCL_SHAPE_WINDOW and PCL_SHAPE_BAND force one (bands need g in
+   [2^-20, 2^20]; outside it the windows run).  Specialised shallow-water module only. */
+#define PCL_SHAPE_AUTO 0
+#define PCL_SHAPE_WINDOW 1
+#define PCL_SHAPE_BAND 2
+int pcl_set_sweep_shape(pcl_ctx* ctx, int eta_shape);
+
 /* ---- mapped (curvilinear) grids ---- */
 
 /* Mesh metrics of a mapped grid, as finalize_mesh leaves them in the reference
@@ -299,7 +308,8 @@ int pcl_batch_download(pcl_batch* batch, int slot, double* vars);
 int pcl_batch_get_step_log(pcl_batch* batch, int slot, pcl_step_record* out, long long cap, long long* n);
 /* Schedule of the persistent kernel (set by the autotuner): rows per mixed work item (0, the
    default: chosen from the instances each time they change), rows per FP64 xi item, rows per FP64
-   eta strip, CTAs per SM (0: the occupancy limit).  Results do not depend on it. */
+   eta item (a chunk of a 4-column band), CTAs per SM (0: the occupancy limit).  Results do not
+   depend on it. */
 int pcl_batch_set_schedule(pcl_batch* batch, int tile_rows, int x_rows, int y_rows, int blocks_per_sm);
 int pcl_batch_info(pcl_batch* batch, int* n_used, int* n_done, long long* cells, long long* device_bytes);
 void* pcl_batch_get_stream(pcl_batch* batch);

@@ -17,6 +17,7 @@ PCL_OK = 0
 PCL_ERR_NAN = -1
 PCL_ERR_NEG_DEPTH = -2
 PCL_ERR_TIMEOUT = -3
+PCL_SHAPE_AUTO, PCL_SHAPE_WINDOW, PCL_SHAPE_BAND = 0, 1, 2  # pcl_set_sweep_shape
 PCL_ERR_OOM = -4
 PCL_ERR_BADARG = -5
 PCL_ERR_CUDA = -6
@@ -108,6 +109,7 @@ def load(build_if_missing: bool = True):
     L.pcl_set_user_bc.argtypes = [vp, vp, vp]
     L.pcl_set_source_hook.argtypes = [vp, vp, vp]
     L.pcl_set_equation.argtypes = [vp, C.c_int, vp, C.c_int]
+    L.pcl_set_sweep_shape.argtypes = [vp, C.c_int]
     L.pcl_compute_mesh_metrics.argtypes = [P(SolverControl), vp, vp, vp, vp, vp]
     L.pcl_update_time.argtypes = [vp, C.c_int]
     L.pcl_set_dt.argtypes = [vp, C.c_double]

@@ -1,9 +1,9 @@
 // batch_fp64.cu -- the FP64 parity step for a batch of grids in one persistent launch.
 //
-// CTAs (128 threads) pull work items from a queue: first every instance's xi-sweep items, then
-// every instance's eta-sweep items.  An eta item waits (bounded) until all xi items of its
-// instance are done.  Those xi items were dequeued before it by CTAs that are running and never
-// wait, so the wait always ends.  The CTA that finishes an instance's last item runs that
+// CTAs (128 threads) pull work items from a queue: first every instance's xi-sweep items (rows
+// of a row segment), then every instance's eta-sweep items (a chunk of rows of a 4-column band).
+// An eta item waits (bounded) until all xi items of its instance are done.  Those xi items were
+// dequeued before it by CTAs that are running and never wait, so the wait always ends.  The CTA that finishes an instance's last item runs that
 // instance's time control (pcl_timectl.cuh) and, if the attempt was accepted, its ghost fill.
 // Per-cell arithmetic is the single-grid kernels' (pcl_sweeps_fp64.cuh): a batched instance is
 // bit-identical to the same grid run alone.  Built with --fmad=false.
@@ -17,55 +17,70 @@
 namespace pcl {
 namespace {
 
-// 128-thread CTAs, 6 per SM (80 registers): measured on B200 with 512 uneven dam breaks, 1.55x
-// the 256-thread, 2-per-SM shape, because both sweeps are latency bound on FP64 division chains.
+// 128-thread CTAs, 8 per SM: both item kinds run the sweeps' shared-memory phases (xi items:
+// rows of a 124-cell segment; eta items: a chunk of rows of a 4-column band, ysweep_band), which
+// fit 64 registers.  The item's grid descriptor is staged in shared memory, so the sweeps read
+// its fields there instead of from a stack copy.
 constexpr int kThreads = 128;
-constexpr int kMinBlocks = 6;
+constexpr int kMinBlocks = 8;
+constexpr int kBandCols = 4;
 
-template <int LIM, bool SO, int MK>
+union BatchSmem {
+  XSmem<kThreads> x;
+  YBSmem<kThreads, kBandCols> y;
+};
+
+template <int LIM, bool SO, int MK, int OPT>
 __device__ __forceinline__ void run_item(const GridDev& g, int kind, int a, int b, const BatchView& v,
-                                         XSmem<kThreads>& S) {
+                                         BatchSmem& S) {
+  double smax = 0.0;
+  int bad = 0;
   if (kind == kItemX) {
     const int jend = min(a + v.x_rows - 1, g.my);
-    double smax = 0.0;
-    int bad = 0;
     for (int j = a; j <= jend; ++j) {
-      xsweep_segment<kThreads, LIM, SO, MK>(g, j, b, S, smax, bad);
+      xsweep_segment<kThreads, LIM, SO, MK, OPT>(g, j, b, S.x, smax, bad);
       __syncthreads();  // the segment's shared arrays are reused by the next row
     }
-    xsweep_finish<kThreads>(g, smax, bad, S);
+    xsweep_finish<kThreads>(g, smax, bad, S.x);
   } else {
-    ysweep_strip<LIM, SO, MK>(g, a, b, v.y_rows);
+    if (!eta_valid(g)) return;  // the same answer for every thread: all xi items are done
+    ysweep_band<kThreads, kBandCols, LIM, SO, MK, OPT>(g, a, b, b + v.y_rows - 1, S.y, smax, bad);
+    block_max_to<kThreads>(&g.ctl->smax_y, smax, S.y.red);
+    if (bad) atomicOr(&g.ctl->status, bad);
   }
 }
 
-template <int MK>
+template <int MK, int OPT>
 __device__ __forceinline__ void dispatch_lim(const GridDev& g, int kind, int a, int b, const BatchView& v,
-                                             XSmem<kThreads>& S) {
-  if (!g.second_order) return run_item<0, false, MK>(g, kind, a, b, v, S);
+                                             BatchSmem& S) {
+  if (!g.second_order) return run_item<0, false, MK, OPT>(g, kind, a, b, v, S);
   switch (g.limiter) {
-    case 1: return run_item<1, true, MK>(g, kind, a, b, v, S);
-    case 2: return run_item<2, true, MK>(g, kind, a, b, v, S);
-    case 3: return run_item<3, true, MK>(g, kind, a, b, v, S);
-    case 4: return run_item<4, true, MK>(g, kind, a, b, v, S);
-    default: return run_item<0, true, MK>(g, kind, a, b, v, S);
+    case 1: return run_item<1, true, MK, OPT>(g, kind, a, b, v, S);
+    case 2: return run_item<2, true, MK, OPT>(g, kind, a, b, v, S);
+    case 3: return run_item<3, true, MK, OPT>(g, kind, a, b, v, S);
+    case 4: return run_item<4, true, MK, OPT>(g, kind, a, b, v, S);
+    default: return run_item<0, true, MK, OPT>(g, kind, a, b, v, S);
   }
 }
 
+// FD: every instance's g lies in the range of the shared-reciprocal quotients (kOptFastDiv,
+// bit-identical to division), chosen by the host per launch.
+template <int FD>
 __device__ __forceinline__ void dispatch_item(const GridDev& g, int kind, int a, int b, const BatchView& v,
-                                              XSmem<kThreads>& S) {
+                                              BatchSmem& S) {
   // batched instances are uniform grids (pcl_batch_add builds the row/column tables)
-  if (g.metric == kMetricUnit) return dispatch_lim<kMetricUnit>(g, kind, a, b, v, S);
-  return dispatch_lim<kMetricTable>(g, kind, a, b, v, S);
+  if (g.metric == kMetricUnit) return dispatch_lim<kMetricUnit, FD ? kOptFastDiv : 0>(g, kind, a, b, v, S);
+  return dispatch_lim<kMetricTable, FD ? kOptFastDiv : 0>(g, kind, a, b, v, S);
 }
 
 // IG: eta items on the edge of their grid fill the ghost cells next to the cells they wrote
 // (ghost_fill_block) and the finishing CTA only the sides left open; else the finishing CTA
 // fills them all.  Separate builds, so the item loop of the IG = false build carries no ghost
 // code.  Same values either way.
-template <bool IG>
+template <bool IG, int FD>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchView v) {
-  __shared__ XSmem<kThreads> S;
+  __shared__ BatchSmem S;
+  __shared__ GridDev sg;
   __shared__ int s_item;
   __shared__ int s_flag;
   const int n = *v.n_items;
@@ -73,10 +88,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
     if (threadIdx.x == 0) s_item = (int)atomicAdd(v.head, 1u);
     __syncthreads();
     const int it = s_item;
-    __syncthreads();
     if (it >= n) break;
     const int4 w = v.items[it];
-    const GridDev g = v.inst[w.x];
+    {  // the item's grid descriptor into shared memory
+      static_assert(sizeof(GridDev) % sizeof(int) == 0, "descriptor copy");
+      const int* src = reinterpret_cast<const int*>(v.inst + w.x);
+      int* dst = reinterpret_cast<int*>(&sg);
+      for (int k = threadIdx.x; k < (int)(sizeof(GridDev) / sizeof(int)); k += kThreads) dst[k] = src[k];
+    }
+    __syncthreads();
+    const GridDev& g = sg;
     Ctl* ctl = g.ctl;
     int* xdone = v.counters + 2 * w.x;
     int* alldone = xdone + 1;
@@ -99,18 +120,18 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
         }
         __syncthreads();
         if (s_flag) {
-          dispatch_item(g, w.y, w.z, w.w, v, S);
+          dispatch_item<FD>(g, w.y, w.z, w.w, v, S);
           if (IG) {
-            const int i1 = min(w.z + kThreads - 1, g.mx), j1 = min(w.w + v.y_rows - 1, g.my);
-            if (w.z == 1 || w.w == 1 || i1 == g.mx || j1 == g.my) {
-              __syncthreads();  // the strip's cells, written by every thread, before any is read
+            const int i0 = max(w.z, 1), i1 = min(w.z + kBandCols - 1, g.mx), j1 = min(w.w + v.y_rows - 1, g.my);
+            if (i0 == 1 || w.w == 1 || i1 == g.mx || j1 == g.my) {
+              __syncthreads();  // the chunk's cells, written by every thread, before any is read
               const int cur = ctl->cur;
-              ghost_fill_block(g, buffer(g, cur == 0 ? 2 : cur - 1), w.z, i1, w.w, j1);
+              ghost_fill_block(g, buffer(g, cur == 0 ? 2 : cur - 1), i0, i1, w.w, j1);
             }
           }
         }
       } else {
-        dispatch_item(g, w.y, w.z, w.w, v, S);
+        dispatch_item<FD>(g, w.y, w.z, w.w, v, S);
       }
     }
     __threadfence();  // every thread's writes of this item precede its completion count
@@ -130,7 +151,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
     if (s_flag && ctl->ierr == 1) {  // update_rank_boundaries of the accepted instance
       double* b = buffer(g, ctl->cur);
       if (IG) {
-        ghost_fill_open_sides(g, b, (g.mx - 1) % kThreads == 0, (g.my - 1) % v.y_rows == 0);
+        // the last band or chunk one cell wide leaves its high side to the finisher
+        const int lb = max(-1 + kBandCols * ((g.mx + 1) / kBandCols), 1);
+        ghost_fill_open_sides(g, b, g.mx - lb + 1 < 2, (g.my - 1) % v.y_rows == 0);
       } else {
         const int ng = ghost_items(g);
         for (int k = threadIdx.x; k < ng; k += blockDim.x) ghost_item(g, b, k);
@@ -140,19 +163,25 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) batch_fp64_kernel(BatchV
   }
 }
 
+template <bool IG, int FD>
+void launch(const BatchView& v, int grid, cudaStream_t st) {
+  batch_fp64_kernel<IG, FD><<<grid, kThreads, 0, st>>>(v);
+}
+
 }  // namespace
 
 void launch_batch_fp64(const BatchView& v, int grid, cudaStream_t st) {
   if (v.item_ghosts)
-    batch_fp64_kernel<true><<<grid, kThreads, 0, st>>>(v);
+    v.fast_div ? launch<true, 1>(v, grid, st) : launch<true, 0>(v, grid, st);
   else
-    batch_fp64_kernel<false><<<grid, kThreads, 0, st>>>(v);
+    v.fast_div ? launch<false, 1>(v, grid, st) : launch<false, 0>(v, grid, st);
 }
 int batch_fp64_threads() { return kThreads; }
 int batch_fp64_segment() { return kThreads - 4; }
+int batch_fp64_band() { return kBandCols; }
 int batch_fp64_occupancy() {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_fp64_kernel<false>, kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_fp64_kernel<false, 1>, kThreads, 0);
   return n > 0 ? n : 1;
 }
 

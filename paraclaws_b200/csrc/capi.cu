@@ -958,6 +958,14 @@ int pcl_set_tile_rows(pcl_ctx* x, int rows) {
   return PCL_OK;
 }
 
+int pcl_set_sweep_shape(pcl_ctx* x, int eta_shape) {
+  if (!x || eta_shape < PCL_SHAPE_AUTO || eta_shape > PCL_SHAPE_BAND) return PCL_ERR_BADARG;
+  static_assert(PCL_SHAPE_WINDOW == kEtaWindow && PCL_SHAPE_BAND == kEtaBand, "shape codes");
+  x->g.eta_shape = eta_shape;
+  drop_graph(x);  // the captured launches run the other kernel
+  return PCL_OK;
+}
+
 int pcl_inject_copy_stall(pcl_ctx* x, int row, unsigned probes) {
   if (!x || !x->mixed || row < -1 || row > x->cfg.m_eta + 2) return PCL_ERR_BADARG;
   mixed_set_injection(x->mixed, row, probes);

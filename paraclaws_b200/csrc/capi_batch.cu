@@ -78,11 +78,12 @@ struct pcl_batch {
   bool dirty = true;
   int n_items = 0;
   // schedule (the autotuner's knobs)
-  int x_rows = 4, y_rows = 16, tile_rows = 0, blocks_per_sm = 0;  // tile_rows 0: chosen per membership
+  int x_rows = 8, y_rows = 128, tile_rows = 0, blocks_per_sm = 0;  // tile_rows 0: chosen per membership
   int tile_rows_eff = 64;  // rows per mixed item in the current items (a launch parameter)
   int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
   int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
   int item_ghosts = 0;  // edge items fill ghost cells (few items per step), else the finisher does
+  int fast_div = 1;     // FP64: every instance's g is inside the shared-reciprocal range
   int launch_ctas = 0;  // CTAs per launch: the persistent grid, or fewer when there are fewer items
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
@@ -131,6 +132,7 @@ static BatchView view(const pcl_batch* b) {
   v.spin_limit = b->spin_limit;
   v.flags = b->scal_d + 2;
   v.stall_slot = b->stall_slot;
+  v.fast_div = b->fast_div;
   return v;
 }
 
@@ -222,9 +224,20 @@ static int rebuild_items(pcl_batch* b) {
     for (int s : order) {
       const auto& c = b->slots[s].cfg;
       int ny = 0;
+      // bands start at column -1 + 4k (sector-aligned rows); the last one holds column m_xi
       for (int j0 = 1; j0 <= c.m_eta; j0 += b->y_rows)
-        for (int i0 = 1; i0 <= c.m_xi; i0 += batch_fp64_threads(), ++ny) items.push_back(make_int4(s, kItemY, i0, j0));
+        for (int i0 = -1; i0 <= c.m_xi; i0 += batch_fp64_band(), ++ny) items.push_back(make_int4(s, kItemY, i0, j0));
       totals[2 * s + 1] = totals[2 * s] + ny;
+    }
+    // the shared-reciprocal quotients' range argument holds for g in [2^-20, 2^20]
+    int fd = 1;
+    for (int s : order) {
+      const double g = b->slots[s].g.grav;
+      if (!(g >= 0x1p-20 && g <= 0x1p20)) fd = 0;
+    }
+    if (!order.empty()) {
+      if (fd != b->fast_div) drop_graph(b);  // a launch parameter of the captured launches
+      b->fast_div = fd;
     }
   }
   if ((long long)items.size() > b->items_cap) {

@@ -14,23 +14,32 @@ namespace pcl {
 // launchers
 // ------------------------------------------------------------------------------------------
 namespace {
-// Launch shapes (measured on B200, 4096^2 bumps after 300 steps, minmod; every variant
+// Launch shapes (measured on B200, bumps after 100-300 steps, minmod; every variant
 // bit-identical): the xi sweep at 8 CTAs of 128 threads per SM, each CTA sweeping 8 rows of its
 // segment with one block reduction at the end, with the shared-reciprocal quotients
-// (kOptFastDiv): 0.391 ms against 0.508 ms for one row per 256-thread CTA at 5 CTAs per SM (4
-// rows: 0.397; the limiter shortcut on top: 0.399).  The eta sweep at 6 CTAs of 128 threads per
-// SM (80 registers, a few spilled window values) with 24-row strips: 0.487 ms (16 rows: 0.492,
-// 32: 0.492).  Measured and dropped for the eta sweep: the two shortcuts and an unrolled row
-// loop (more registers, more spills); the xi sweep's shared-memory phases run along the columns
-// of 4-column tiles (0.516 ms at best); and an xi sweep that stores its result transposed so the
-// eta sweep can read contiguous lines (0.645 + 0.653 ms: the strided stores cost more than the
-// phases save).
+// (kOptFastDiv): 0.391 ms at 4096^2 against 0.508 ms for one row per 256-thread CTA at 5 CTAs
+// per SM (4 rows: 0.397; the limiter shortcut on top: 0.399).
+// The eta sweep has two shapes.  Column windows (ysweep_strip) at 6 CTAs of 128 threads per SM
+// (80 registers, a few spilled window values) with 24-row strips: 0.487 ms at 4096^2 (16 rows:
+// 0.492, 32: 0.492), 1.73 ms at 8192^2.  Bands of 4 columns (ysweep_band) in 256-row chunks at 8
+// CTAs per SM (64 registers, no spills): 0.046 ms at 1024^2 against 0.060 for the best window
+// strip, 0.157 against 0.170 at 2048^2, 0.504 against 0.487 at 4096^2.  Windows where they fill
+// the GPU with at least kYWaves waves of CTAs, bands below that.  Measured and dropped for the
+// eta sweep: the two shortcuts and an unrolled row loop in the windows (more registers, more
+// spills); tiles that recompute their 4 halo rows instead of carrying them (0.489 ms at best);
+// and an xi sweep that stores its result transposed so the eta sweep can read contiguous lines
+// (0.645 + 0.653 ms: the strided stores cost more than the phases save).
 constexpr int kXT = 128;   // threads (and slots) of an xi-sweep CTA
 constexpr int kXMinBlocks = 8;
 constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA
-constexpr int kYT = 128;   // columns of an eta-sweep CTA
+constexpr int kYT = 128;   // columns of an eta-sweep window CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 24;    // rows of an eta-sweep strip
+constexpr int kBT = 128;   // threads of an eta-sweep band CTA
+constexpr int kBX = 4;     // columns of a band
+constexpr int kBMinBlocks = 8;
+constexpr int kBChunk = 256;  // rows of a band CTA
+constexpr int kYWaves = 4;
 
 // A CTA sweeps R consecutive rows of one segment (blockIdx.y*R ..), strided by gridDim.y*R
 // when the grid has more rows than one launch's blocks cover.
@@ -56,6 +65,18 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
   ysweep_strip<LIM, SO, MK>(g, 1 + blockIdx.x * NTX, 1 + blockIdx.y * STRIP, STRIP);
 }
 
+template <int LIM, bool SO, int MK>
+__global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g) {
+  __shared__ YBSmem<kBT, kBX> S;
+  if (g.ctl->done || !eta_valid(g)) return;
+  double smax = 0.0;
+  int bad = 0;
+  const int j0 = 1 + blockIdx.y * kBChunk;
+  ysweep_band<kBT, kBX, LIM, SO, MK, kOptFastDiv>(g, -1 + blockIdx.x * kBX, j0, j0 + kBChunk - 1, S, smax, bad);
+  block_max_to<kBT>(&g.ctl->smax_y, smax, S.red);
+  if (bad) atomicOr(&g.ctl->status, bad);
+}
+
 // The shortcuts' range argument assumes g in [2^-20, 2^20] (pcl_fp64.cuh: kOptFastDiv).
 inline bool fast_div_ok(const GridDev& g) { return g.grav >= 0x1p-20 && g.grav <= 0x1p20; }
 
@@ -68,10 +89,27 @@ void launch_x_t(const GridDev& g, cudaStream_t st) {
   else
     xsweep_fp64_kernel<kXT, LIM, SO, MK, kXRows><<<gx, kXT, 0, st>>>(g);
 }
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
 template <int LIM, bool SO, int MK>
 void launch_y_t(const GridDev& g, cudaStream_t st) {
   dim3 gy((g.mx + kYT - 1) / kYT, (g.my + kYS - 1) / kYS);
-  ysweep_fp64_kernel<kYT, kYS, LIM, SO, MK><<<gy, kYT, 0, st>>>(g);
+  const bool band = g.eta_shape == kEtaBand ||
+                    (g.eta_shape == kEtaAuto && (long long)gy.x * gy.y < (long long)kYWaves * kYMinBlocks * sm_count());
+  if (band && fast_div_ok(g)) {
+    dim3 gb((g.mx + 2 + kBX - 1) / kBX, (g.my + kBChunk - 1) / kBChunk);
+    yband_fp64_kernel<LIM, SO, MK><<<gb, kBT, 0, st>>>(g);
+  } else {
+    ysweep_fp64_kernel<kYT, kYS, LIM, SO, MK><<<gy, kYT, 0, st>>>(g);
+  }
 }
 template <template <int, bool, int> class F, int MK>
 void dispatch_lim(const GridDev& g, cudaStream_t st) {

@@ -4,7 +4,8 @@
 // Work items (int4 {slot, kind, a, b}), read from device memory so the batch can change between
 // launches without re-capturing the CUDA graph:
 //   kind kItemX     FP64 xi sweep of rows a .. a+rows-1 of the segment starting at column b
-//   kind kItemY     FP64 eta sweep of the columns from a, strip of rows from b
+//   kind kItemY     FP64 eta sweep of the 4-column band from column a (-1 + 4k), rows b ..
+//                   b+rows-1
 //   kind kItemMixed mixed-precision fused item: strip a, row segment b
 // Per instance, counters[2*slot] counts finished xi items (eta items of that instance wait for
 // all of them) and counters[2*slot+1] all finished items; the CTA that finishes the last item
@@ -48,6 +49,7 @@ struct BatchView {
   int* flags;            // device scalar: bit 0 set when any bounded wait of the launch gave up
   int stall_slot;        // test of the timeout path (-1: off): the eta items of this slot wait
                          // for one xi item more than the step has, so their wait runs out
+  int fast_div;          // FP64: every instance's g is inside the shared-reciprocal range
 };
 
 void launch_batch_fp64(const BatchView& v, int grid, cudaStream_t st);
@@ -61,8 +63,9 @@ cudaError_t batch_mixed_set_desc(int index, const ItemDesc& d, cudaStream_t st);
 // there is no room; release them again
 int batch_desc_reserve(int n);
 void batch_desc_release(int base, int n);
-int batch_fp64_threads();   // also the columns of an FP64 eta item
+int batch_fp64_threads();
 int batch_fp64_segment();   // cells of an FP64 xi item's row segment
+int batch_fp64_band();      // columns of an FP64 eta item's band
 int batch_mixed_threads();
 // largest number of resident CTAs per SM of each persistent kernel
 int batch_fp64_occupancy();

@@ -195,6 +195,16 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
   }
 }
 
+// xi-sweep validity (MOD_solve.f90:107-120), recomputed from the xi sweep's reduction word
+__device__ __forceinline__ bool eta_valid(const GridDev& g) {
+  const Ctl* ctl = g.ctl;
+  // written by atomics of other CTAs in a batched launch: read at L2, not a stale L1 line
+  const double sx = __longlong_as_double((long long)__ldcg(&ctl->smax_x));
+  const double cflx = sx * ctl->dt / g.dxi;
+  const double cfl = fmax(ctl->CFL, cflx);
+  return ctl->CFL_target / cfl >= ctl->shrink;
+}
+
 // ------------------------------------------------------------------------------------------
 // eta sweep.  One thread = one column i, marching over a strip of rows [j0, j1] with a
 // register window of three interfaces.  Loads of consecutive threads are consecutive doubles.
@@ -235,14 +245,7 @@ template <int LIM, bool SO, int MK = kMetricTable, int OPT = 0, int UNR = 1>
 __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0, int strip_rows) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   Ctl* ctl = g.ctl;
-  // xi-sweep validity (MOD_solve.f90:107-120), recomputed here from the reduction word
-  {
-    // written by atomics of other CTAs in a batched launch: read at L2, not a stale L1 line
-    const double sx = __longlong_as_double((long long)__ldcg(&ctl->smax_x));
-    const double cflx = sx * ctl->dt / g.dxi;
-    const double cfl = fmax(ctl->CFL, cflx);
-    if (!(ctl->CFL_target / cfl >= ctl->shrink)) return;
-  }
+  if (!eta_valid(g)) return;
   const int cur = ctl->cur;
   const int xb = cur == 2 ? 0 : cur + 1;
   const int yb = cur == 0 ? 2 : cur - 1;
@@ -352,6 +355,204 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
   smax = warp_max(smax);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&ctl->smax_y, smax);
   if (bad) atomicOr(&ctl->status, bad);
+}
+
+// ------------------------------------------------------------------------------------------
+// eta sweep in bands (the shape for grids too small to fill the GPU with column windows).  A CTA
+// walks down a band of TX columns over rows j0 .. j1 in steps of L = NT/TX rows, running the xi
+// sweep's four shared-memory phases along the columns: slot (r, c) = (row, column in the band),
+// so a warp's loads are TX*8 contiguous bytes on each of 32/TX rows.  The last two cells, the last
+// two interfaces and the last correction flux of a step stay in history slots (rows 0, 1) for the
+// next step, so only the four rows in front of j0 are computed twice.  Bands start at column
+// i = -1 + TX*k (a 32-byte sector boundary, the pitch being a multiple of 32 doubles); columns
+// outside 1 .. m_xi are computed on a clamped column and written nowhere.
+//
+// Semantics of ysweep_strip: rows 1 .. m_eta from the xi-swept buffer, the ghost rows from the
+// pre-step buffer (main.f90:210 runs before the ghost fill at :246); getJakobi's status over rows -1 .. m_eta+1; waves of interfaces beyond
+// m_eta+1 are zero and the interface m_eta+1 is unlimited; the pre-step ghost cells carried into
+// the new buffer.  The first step of a CTA starts at s = j0-2 with empty history: its interface
+// s and the correction fluxes and updates that would read the history are never used (updates
+// start at row j0).  The caller checks the xi-sweep validity (eta_valid) and reduces smax and
+// the status bits over the CTA.
+// ------------------------------------------------------------------------------------------
+template <int NT, int TX>
+struct YBSmem {
+  static constexpr int L = NT / TX;
+  double sq[3][(L + 2) * TX], sf[3][(L + 2) * TX], ss[(L + 2) * TX], sk[(L + 2) * TX], slr[(L + 2) * TX];
+  double sw1[3][(L + 2) * TX], sw2[3][(L + 2) * TX], ss2[(L + 2) * TX];
+  double sft[3][(L + 1) * TX];
+  double red[NT / 32];
+  bool sok[(L + 2) * TX];
+};
+
+template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
+__device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1, YBSmem<NT, TX>& S,
+                                            double& smax_acc, int& bad_acc) {
+  constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
+  constexpr int L = NT / TX;
+  const Ctl* ctl = g.ctl;
+  const int cur = ctl->cur;
+  const int xb = cur == 2 ? 0 : cur + 1;
+  const int yb = cur == 0 ? 2 : cur - 1;
+  const double dtod = ctl->dtod_y;
+  const int mx = g.mx, my = g.my;
+  const long long P = g.pitch;
+  const int t = threadIdx.x;
+  const int cx = t % TX, r = t / TX;
+  const int i = i0 + cx;
+  const bool active = i >= 1 && i <= mx;
+  const int ic = i < 1 ? 1 : (i > mx ? mx : i);
+  const double* pre = buffer(g, cur);
+  const double* xsw = buffer(g, xb);
+  double* outp = buffer(g, yb);
+  const double gam = (UM || MP) ? 1.0 : __ldg(g.colm + (ic + 1) * kColMetrics + 2);
+  double smax = 0.0;
+  int bad = 0;
+  const int jlast = min(j1, my);
+
+  for (int s = j0 - 2; s - 2 <= jlast; s += L) {
+    {  // phase A: cell j = s + r into slot (r+2)TX + c
+      const int j = s + r;
+      const int sl = (r + 2) * TX + cx;
+      if (j <= my + 2) {
+        const double* src = (j >= 1 && j <= my) ? xsw : pre;
+        const long long o = (long long)(j + 1) * P + (ic + 1);
+        const double h = src[o], hu = src[o + g.plane], hv = src[o + 2 * g.plane];
+        int cb = 0;
+        const CellFlux F = cell_flux<1, OPT>(h, hu, hv, g.grav, &cb);
+        if (j <= my + 1 && active) bad |= cb;
+        S.sq[0][sl] = h; S.sq[1][sl] = hu; S.sq[2][sl] = hv;
+        S.sf[0][sl] = F.f0; S.sf[1][sl] = F.f1; S.sf[2][sl] = F.f2;
+        S.ss[sl] = F.s;
+        if constexpr ((OPT & kOptFastDiv) != 0) S.sok[sl] = F.ok;
+        if constexpr (MP) {
+          S.sk[sl] = __ldg(g.kap + o);
+          S.slr[sl] = __ldg(g.lry + o);
+        } else if constexpr (!UM) {
+          S.sk[sl] = capacity(g.rowm, g.colm, ic, j, g.area_scale);
+        }
+      }
+    }
+    __syncthreads();
+    {  // phase B: interface k = s + r (cells k-1, k) into slot (r+2)TX + c
+      const int k = s + r;
+      const int sl = (r + 2) * TX + cx, sm = sl - TX;
+      Waves W;
+      double s2 = 0.0;
+      if (k <= my + 1 && k >= j0 - 1) {
+        const double qL[3] = {S.sq[0][sm], S.sq[1][sm], S.sq[2][sm]};
+        const double qR[3] = {S.sq[0][sl], S.sq[1][sl], S.sq[2][sl]};
+        CellFlux FL = {S.sf[0][sm], S.sf[1][sm], S.sf[2][sm], S.ss[sm]};
+        CellFlux FR = {S.sf[0][sl], S.sf[1][sl], S.sf[2][sl], S.ss[sl]};
+        if constexpr ((OPT & kOptFastDiv) != 0) FL.ok = S.sok[sm], FR.ok = S.sok[sl];
+        s2 = hll<OPT>(qL, FL, qR, FR, W);
+        if (active) smax = fmax(smax, s2);
+      } else {
+#pragma unroll
+        for (int me = 0; me < 3; ++me) W.w1[me] = W.w2[me] = 0.0;
+      }
+#pragma unroll
+      for (int me = 0; me < 3; ++me) {
+        S.sw1[me][sl] = W.w1[me];
+        S.sw2[me][sl] = W.w2[me];
+      }
+      S.ss2[sl] = s2;
+    }
+    __syncthreads();
+    if constexpr (SO) {  // phase C: correction flux at interface k = s - 1 + r into ft slot (r+1)TX + c
+      const int k = s - 1 + r;
+      const int w = (r + 1) * TX + cx;  // interface k's slot; k-1 at w - TX, k+1 at w + TX
+      double ft[3] = {0.0, 0.0, 0.0};
+      if (k <= my + 1) {
+        const double s2 = S.ss2[w];
+        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, S.sk[w - TX], S.sk[w]);
+        if (cf != 0.0) {
+          const double w1[3] = {S.sw1[0][w], S.sw1[1][w], S.sw1[2][w]};
+          const double w2[3] = {S.sw2[0][w], S.sw2[1][w], S.sw2[2][w]};
+          double a[3], b[3];
+          if (LIM != 0 && k <= my) {
+            const double w1m[3] = {S.sw1[0][w - TX], S.sw1[1][w - TX], S.sw1[2][w - TX]};
+            const double w1p[3] = {S.sw1[0][w + TX], S.sw1[1][w + TX], S.sw1[2][w + TX]};
+            const double w2m[3] = {S.sw2[0][w - TX], S.sw2[1][w - TX], S.sw2[2][w - TX]};
+            const double w2p[3] = {S.sw2[0][w + TX], S.sw2[1][w + TX], S.sw2[2][w + TX]};
+            limit_wave<LIM, OPT>(w1m, w1, w1p, false, a);
+            limit_wave<LIM, OPT>(w2m, w2, w2p, s2 > 0.0, b);
+          } else {
+#pragma unroll
+            for (int me = 0; me < 3; ++me) {
+              a[me] = w1[me];
+              b[me] = w2[me];
+            }
+          }
+#pragma unroll
+          for (int me = 0; me < 3; ++me) ft[me] = cf * a[me] + cf * b[me];
+        }
+      }
+#pragma unroll
+      for (int me = 0; me < 3; ++me) S.sft[me][(r + 1) * TX + cx] = ft[me];
+    }
+    __syncthreads();
+    {  // phase D: update of cell j = s - 2 + r (cell and interface slot rTX + c)
+      const int j = s - 2 + r;
+      if (active && j >= j0 && j <= jlast) {
+        const int c = r * TX + cx;
+        const double gl = MP ? S.slr[c] : gam;
+        const double gr = MP ? S.slr[c + TX] : gam;
+        const double dtk = UM ? dtod : dtod / S.sk[c];
+        const double sp = S.ss2[c];
+        const double sm = -S.ss2[c + TX];
+        const long long o = (long long)(j + 1) * P + (i + 1);
+#pragma unroll
+        for (int me = 0; me < 3; ++me) {
+          const double ap = sp * S.sw2[me][c];
+          const double am = sm * S.sw1[me][c + TX];
+          double q = UM ? S.sq[me][c] - dtk * (ap + am) : S.sq[me][c] - dtk * (gl * ap + gr * am);
+          if constexpr (SO) q = q - dtk * (S.sft[me][c + TX] - S.sft[me][c]);
+          outp[o + me * g.plane] = q;
+        }
+        if (i == 1 || i == mx) {  // the pre-step ghost columns beside the edge columns
+          const long long ob = (long long)(j + 1) * P;
+          const int g0 = i == 1 ? -1 : mx + 1;
+#pragma unroll
+          for (int gcol = g0; gcol <= g0 + 1; ++gcol)
+#pragma unroll
+            for (int me = 0; me < 3; ++me) outp[ob + gcol + 1 + me * g.plane] = pre[ob + gcol + 1 + me * g.plane];
+        }
+      }
+    }
+    __syncthreads();
+    if (r < 2) {  // history: cells and interfaces of rows L, L+1 -> 0, 1; correction flux L -> 0
+      const int from = (L + r) * TX + cx, to = r * TX + cx;
+#pragma unroll
+      for (int me = 0; me < 3; ++me) {
+        S.sq[me][to] = S.sq[me][from];
+        S.sf[me][to] = S.sf[me][from];
+        S.sw1[me][to] = S.sw1[me][from];
+        S.sw2[me][to] = S.sw2[me][from];
+      }
+      S.ss[to] = S.ss[from];
+      S.ss2[to] = S.ss2[from];
+      if constexpr ((OPT & kOptFastDiv) != 0) S.sok[to] = S.sok[from];
+      if constexpr (MP) S.slr[to] = S.slr[from];
+      if constexpr (MP || !UM) S.sk[to] = S.sk[from];
+      if (r == 0) {
+#pragma unroll
+        for (int me = 0; me < 3; ++me) S.sft[me][cx] = S.sft[me][L * TX + cx];
+      }
+    }
+    __syncthreads();
+  }
+  if (active && r < 4) {  // the pre-step ghost rows of the band's columns
+    auto copy_cell = [&](int ci, int cj) {
+      const long long o = (long long)(cj + 1) * P + (ci + 1);
+#pragma unroll
+      for (int me = 0; me < 3; ++me) outp[o + me * g.plane] = pre[o + me * g.plane];
+    };
+    if (r < 2 && j0 == 1) copy_cell(i, -1 + r);
+    if (r >= 2 && jlast == my) copy_cell(i, my + r - 1);
+  }
+  smax_acc = fmax(smax_acc, smax);
+  bad_acc |= bad;
 }
 
 }  // namespace pcl

@@ -43,6 +43,11 @@ enum : int { kPrecFP64 = 0, kPrecMixed = 1 };
 //                 length_ratio_xi(1,:,:), length_ratio_eta(1,:,:))
 enum : int { kMetricTable = 0, kMetricUnit = 1, kMetricMapped = 2 };
 
+// Shape of the FP64 eta sweep (same results for every shape): chosen by grid size, or forced
+// (pcl_set_sweep_shape).  Column windows: one thread per column over a strip of rows; bands:
+// shared-memory phases along the columns of 4-column bands.
+enum : int { kEtaAuto = 0, kEtaWindow = 1, kEtaBand = 2 };
+
 struct StepLogEntry {   // one attempted step, as main.f90 prints it
   double dt;            // dt used by the attempt
   double cfl;           // CFL of the attempt (t_ctrl%CFL before reset_CFL)
@@ -99,6 +104,7 @@ struct GridDev {
                              // -1: none chosen yet (contexts of num_equations != 3)
   int neq;                   // planes per buffer: num_equations (3 for every path but the generic one)
   double eqp[2];             // its parameters (shallow water: g)
+  int eta_shape;             // kEta*: the FP64 eta sweep's shape
   double dxi, deta, area_scale /* d_xi*d_eta */, grav;
   // kMetricMapped only: per-cell metrics, cell (i, j) at [(j+1)*pitch + (i+1)]
   const double* kap;         // capacity(i, j)

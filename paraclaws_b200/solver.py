@@ -211,6 +211,10 @@ class Solver:
         _lib.check(self.L.pcl_set_equation(self.h, int(module), arr if params else None, len(params)),
                    "pcl_set_equation")
 
+    def set_sweep_shape(self, eta_shape: int) -> None:
+        """Shape of the FP64 eta sweep (_lib.PCL_SHAPE_*): a schedule, the results stay the same."""
+        _lib.check(self.L.pcl_set_sweep_shape(self.h, int(eta_shape)), "pcl_set_sweep_shape")
+
     def set_source_hook(self, fn_address: Optional[int], user: Optional[int] = None) -> None:
         """Install a pcl_source_fn (integrate_source_term with a non-zero phi); None: phi = 0."""
         _lib.check(self.L.pcl_set_source_hook(self.h, fn_address, user), "pcl_set_source_hook")
