@@ -512,7 +512,7 @@ def _run_to_completion(b, torch):
     return e0.elapsed_time(e1), attempts
 
 
-def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), l1=True):
+def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), l1=True, side=0):
     """C4: 512 dam-break instances, each with its own adaptive dt, run to 200 accepted steps each
     in one persistent launch per attempted step (CUDA graphs of 16), after the autotuner picked
     the schedule on a separate copy of the batch.  Work = sum over instances of m^2 x accepted
@@ -525,6 +525,8 @@ def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), 
     from paraclaws_b200 import control as ctl
     from paraclaws_b200.batch import autotune
     sides, params = batch_instances(n)
+    if side > 0:  # profiling: n instances of one size
+        sides = [side] * n
     peak, _ = hbm_peak()
     res = {}
     finals = {}
@@ -582,7 +584,8 @@ def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), 
     res["cells"] = int(sum(m * m for m in sides))
     res["launches_per_step"] = 1
     res["workload"] = (f"C4: {n} dam breaks, sides log-uniform 64..1024 (multiples of 32, seed 2), seeded dams, "
-                       f"minmod, walls, CFL 0.9, {accepted_steps} accepted steps each")
+                       f"minmod, walls, CFL 0.9, {accepted_steps} accepted steps each") if side <= 0 else (
+        f"{n} dam breaks of {side}^2, seeded dams, minmod, walls, CFL 0.9, {accepted_steps} accepted steps each")
     return res
 
 
@@ -857,6 +860,8 @@ def main():
     ap.add_argument("--form", choices=["batch"], help="run only this form and print its result (profiling)")
     ap.add_argument("--instances", type=int, default=512, help="--form batch: number of grids")
     ap.add_argument("--batch-precision", choices=["fp64", "mixed", "both"], default="both")
+    ap.add_argument("--batch-side", type=int, default=0, help="--form batch: every grid this size (profiling)")
+    ap.add_argument("--batch-steps", type=int, default=200, help="--form batch: accepted steps per grid")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -864,7 +869,8 @@ def main():
         import torch
         torch.cuda.set_device(0)
         prec = ("fp64", "mixed") if args.batch_precision == "both" else (args.batch_precision,)
-        print(json.dumps({"form": "batch", **form_batch(0, n=args.instances, precisions=prec)}), flush=True)
+        print(json.dumps({"form": "batch", **form_batch(0, n=args.instances, precisions=prec, side=args.batch_side,
+                                                        accepted_steps=args.batch_steps)}), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:

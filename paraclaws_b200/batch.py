@@ -136,7 +136,7 @@ class Batch:
 def candidate_schedules(precision: int) -> List[Schedule]:
     if precision == PRECISION_MIXED:
         return [Schedule(tile_rows=tr, blocks_per_sm=b) for tr in (0, 32, 64, 128, 256) for b in (0, 3)]
-    return [Schedule(x_rows=xr, y_rows=yr, blocks_per_sm=b) for xr in (4, 8, 16) for yr in (32, 64, 128, 256)
+    return [Schedule(x_rows=xr, y_rows=yr, blocks_per_sm=b) for xr in (8, 16) for yr in (64, 128, 256, 512)
             for b in (0, 6)]
 
 

@@ -390,6 +390,7 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
                                             double& smax_acc, int& bad_acc) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   constexpr int L = NT / TX;
+  static_assert(NT % 32 == 0 && TX <= 16 && L >= 4, "band shape: rows 0, 1 within warp 0");
   const Ctl* ctl = g.ctl;
   const int cur = ctl->cur;
   const int xb = cur == 2 ? 0 : cur + 1;
@@ -520,8 +521,12 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
         }
       }
     }
-    __syncthreads();
-    if (r < 2) {  // history: cells and interfaces of rows L, L+1 -> 0, 1; correction flux L -> 0
+    // History: cells and interfaces of rows L, L+1 -> 0, 1, correction flux L -> 0.  Phase D
+    // reads rows 0 and 1 of those arrays only in threads r = 0, 1 (row 2 and up belong to
+    // later rows), which share warp 0 with the copying threads (32/TX >= 2 rows per warp): a
+    // warp barrier orders them.  The rows copied from were final before phase D.
+    if (threadIdx.x < 32) __syncwarp();
+    if (r < 2) {
       const int from = (L + r) * TX + cx, to = r * TX + cx;
 #pragma unroll
       for (int me = 0; me < 3; ++me) {
