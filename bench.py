@@ -471,9 +471,10 @@ def batch_instances(n: int = 512, seed: int = 2):
     return sides, [ic.seeded_dam_params(k, offset=0.25) for k in range(n)]
 
 
-def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None):
-    """One batch of the C4 instances, each stopping after `accepted_steps` accepted steps.  With
-    perturb_seed, the FP64 start has h raised by one ulp in 1% of the cells (host-built state)."""
+def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None, time_finals=None):
+    """One batch of the C4 instances, each stopping after `accepted_steps` accepted steps (0: at
+    its time_final, from `time_finals`, else never).  With perturb_seed, the FP64 start has h
+    raised by one ulp in 1% of the cells (host-built state)."""
     import numpy as np
 
     from paraclaws_b200 import control as ctl
@@ -481,15 +482,18 @@ def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None):
     from paraclaws_b200.batch import Batch
     b = Batch(len(sides), precision=prec, device=device)
     rng = np.random.Generator(np.random.PCG64(perturb_seed)) if perturb_seed is not None else None
-    for m, p in zip(sides, params):
+    for k, (m, p) in enumerate(zip(sides, params)):
         cu = ctl.CustomSettings(precision_mode=prec, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out,
                                 dam_x0=p.x0, dam_y0=p.y0, max_accepted_steps=accepted_steps)
+        tf = float(time_finals[k]) if time_finals is not None else 1.0e9
         q = None
         if rng is not None:
             q = ic.circular_dam(m, m, p.radius, p.h_in, p.h_out, p.x0, p.y0)
             mask = rng.random(q.shape[:2]) < 0.01
             q[..., 0] = np.where(mask, np.nextafter(q[..., 0], np.inf), q[..., 0])
-        b.add(ctl.dam_break_control(m, limiter=1, bc=1, time_final=1.0e9), q, cu)
+        # one snapshot time, the end: a clamp onto an intermediate snapshot time shortens a step by
+        # however close the run happens to be to it, and dt regrows only 1.2x per step after that
+        b.add(ctl.dam_break_control(m, limiter=1, bc=1, time_final=tf, number_of_snapshots=1), q, cu)
     return b
 
 
@@ -578,6 +582,35 @@ def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), 
                                           "of_mixed_max_instance: the floor of the instance where mixed is "
                                           "furthest from FP64 (an instance that amplifies any perturbation "
                                           "shows it in both)"}
+        # The same comparison at the same physical time: after equal accepted-step counts the two
+        # runs can stand at different times (a near-tie of the largest wave speed between two cells
+        # resolved one step apart gives different dt sequences).  Each instance runs again in both
+        # precisions to the time its FP64 run reached, the last step clamped onto it (the FP64 run
+        # repeats its accepted steps exactly).
+        t_end = [finals["fp64"].stats(k).time for k in range(n)]
+        same = {}
+        for name, prec, pert in (("fp64", ctl.PRECISION_FP64, None), ("mixed", ctl.PRECISION_MIXED, None),
+                                 ("fp64_perturbed", ctl.PRECISION_FP64, 7)):
+            bb = _make_batch(prec, sides, params, device, 0, perturb_seed=pert, time_finals=t_end)
+            _run_to_completion(bb, torch)
+            same[name] = bb
+        l1_t, fl_t, dt_end = [], [], []
+        for k in range(n):
+            ref = same["fp64"].download(k)[2:-2, 2:-2, 0]
+            scale = float(np.abs(ref).sum())
+            l1_t.append(float(np.abs(same["mixed"].download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
+            fl_t.append(float(np.abs(same["fp64_perturbed"].download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
+            dt_end.append(abs(same["mixed"].stats(k).time - same["fp64"].stats(k).time))
+        for bb in same.values():
+            bb.close()
+        worst_t = int(np.argmax(l1_t))
+        res["l1_h_mixed_vs_fp64_same_time"] = {
+            "median": float(np.median(l1_t)), "p99": float(np.percentile(l1_t, 99)), "max": float(max(l1_t)),
+            "max_instance": worst_t, "max_instance_side": int(sides[worst_t]),
+            "instances_le_1e-5": int(sum(v <= 1e-5 for v in l1_t)),
+            "fp64_floor_median": float(np.median(fl_t)), "fp64_floor_max": float(max(fl_t)),
+            "end_time_diff_max": float(max(dt_end)),
+            "note": "both precisions run to the time the FP64 instance reached after the accepted steps"}
     for b in finals.values():
         b.close()
     res["instances"] = n
@@ -654,6 +687,7 @@ def target_summary(fp64_value: float, forms: dict) -> dict:
     mx = b.get("mixed", {})
     l1 = b.get("l1_h_mixed_vs_fp64", {})
     fl = b.get("l1_h_fp64_floor", {})
+    lt = b.get("l1_h_mixed_vs_fp64_same_time", {})
     srv = forms.get("serving", {})
 
     def serve(name, rate):
@@ -671,11 +705,14 @@ def target_summary(fp64_value: float, forms: dict) -> dict:
          "l1_h_fp64_floor_median": _sig(fl.get("median")),
          "l1_h_le_1e-5_instances": l1.get("instances_le_1e-5"),
          "l1_h_fp64_floor_of_max_instance": _sig(fl.get("of_mixed_max_instance")),
+         "l1_h_same_time_median": _sig(lt.get("median")), "l1_h_same_time_max": _sig(lt.get("max")),
+         "l1_h_same_time_le_1e-5_instances": lt.get("instances_le_1e-5"),
          "serving_mixed": serve("mixed", 12.0), "serving_fp64": serve("fp64", 3.0),
          "workload": "C4, 512 instances x 200 accepted steps; serving C5"}
     if v:
         t["met"] = {"speedup_ge_2": v / fp64_value >= 2.0, "effective_roofline_ge_0.70": mx["effective_roofline_frac"] >= 0.7,
-                    "l1_h_max_le_1e-5": bool(l1) and l1["max"] <= 1e-5}
+                    "l1_h_max_le_1e-5": bool(l1) and l1["max"] <= 1e-5,
+                    "l1_h_same_time_max_le_1e-5": bool(lt) and lt["max"] <= 1e-5}
     return t
 
 
@@ -745,7 +782,9 @@ def run_ours(args) -> None:
     s.advance(max_attempts=args.warmup)
     kms = s.profile_kernels(reps=10)
     if prec == ctl.PRECISION_FP64:
-        names = ["xsweep_fp64", "ysweep_fp64", "timectl", "ghost"]
+        from paraclaws_b200 import _lib
+        eta = "yband_fp64" if s.sweep_shape() == _lib.PCL_SHAPE_BAND else "ysweep_fp64"
+        names = ["xsweep_fp64", eta, "timectl", "ghost"]
         sweep_ms = {names[0]: kms[0], names[1]: kms[1]}
         bytes_per_launch = BYTES_PER_CELL_SWEEP * m * m
     else:

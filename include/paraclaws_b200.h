@@ -201,6 +201,9 @@ int pcl_set_equation(pcl_ctx* ctx, int module, const double* params, int nparams
 #define PCL_SHAPE_WINDOW 1
 #define PCL_SHAPE_BAND 2
 int pcl_set_sweep_shape(pcl_ctx* ctx, int eta_shape);
+/* The shape the FP64 eta sweep runs for this context's grid (PCL_SHAPE_WINDOW or
+   PCL_SHAPE_BAND), with PCL_SHAPE_AUTO resolved. */
+int pcl_get_sweep_shape(pcl_ctx* ctx, int* eta_shape);
 
 /* ---- mapped (curvilinear) grids ---- */
 

@@ -110,6 +110,7 @@ def load(build_if_missing: bool = True):
     L.pcl_set_source_hook.argtypes = [vp, vp, vp]
     L.pcl_set_equation.argtypes = [vp, C.c_int, vp, C.c_int]
     L.pcl_set_sweep_shape.argtypes = [vp, C.c_int]
+    L.pcl_get_sweep_shape.argtypes = [vp, P(C.c_int)]
     L.pcl_compute_mesh_metrics.argtypes = [P(SolverControl), vp, vp, vp, vp, vp]
     L.pcl_update_time.argtypes = [vp, C.c_int]
     L.pcl_set_dt.argtypes = [vp, C.c_double]

@@ -27,7 +27,7 @@ constexpr int kBandCols = 4;
 
 union BatchSmem {
   XSmem<kThreads> x;
-  YBSmem<kThreads, kBandCols> y;
+  YBSmem<kThreads, kBandCols, false> y;
 };
 
 template <int LIM, bool SO, int MK, int OPT>

@@ -966,6 +966,12 @@ int pcl_set_sweep_shape(pcl_ctx* x, int eta_shape) {
   return PCL_OK;
 }
 
+int pcl_get_sweep_shape(pcl_ctx* x, int* eta_shape) {
+  if (!x || !eta_shape) return PCL_ERR_BADARG;
+  *eta_shape = eta_shape_of(x->g);
+  return PCL_OK;
+}
+
 int pcl_inject_copy_stall(pcl_ctx* x, int row, unsigned probes) {
   if (!x || !x->mixed || row < -1 || row > x->cfg.m_eta + 2) return PCL_ERR_BADARG;
   mixed_set_injection(x->mixed, row, probes);

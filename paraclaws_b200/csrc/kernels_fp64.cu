@@ -20,15 +20,20 @@ namespace {
 // (kOptFastDiv): 0.391 ms at 4096^2 against 0.508 ms for one row per 256-thread CTA at 5 CTAs
 // per SM (4 rows: 0.397; the limiter shortcut on top: 0.399).
 // The eta sweep has two shapes.  Column windows (ysweep_strip) at 6 CTAs of 128 threads per SM
-// (80 registers, a few spilled window values) with 24-row strips: 0.487 ms at 4096^2 (16 rows:
-// 0.492, 32: 0.492), 1.73 ms at 8192^2.  Bands of 4 columns (ysweep_band) in 256-row chunks at 8
-// CTAs per SM (64 registers, no spills): 0.046 ms at 1024^2 against 0.060 for the best window
-// strip, 0.157 against 0.170 at 2048^2, 0.504 against 0.487 at 4096^2.  Windows where they fill
-// the GPU with at least kYWaves waves of CTAs, bands below that.  Measured and dropped for the
-// eta sweep: the two shortcuts and an unrolled row loop in the windows (more registers, more
-// spills); tiles that recompute their 4 halo rows instead of carrying them (0.489 ms at best);
-// and an xi sweep that stores its result transposed so the eta sweep can read contiguous lines
-// (0.645 + 0.653 ms: the strided stores cost more than the phases save).
+// (80 registers, a few spilled window values) with 24-row strips (16 rows: +1%, 32: +1%).  Bands
+// of 8 columns (ysweep_band) at 8 CTAs per SM (64 registers, no spills), each thread staging its
+// cell of the next 16-row step by cp.async while the phases of this one run.  Eta sweep in ms
+// on bumps after 8 / 200 steps, windows against bands: 4096^2 0.482 / 0.499 against 0.465 /
+// 0.468 (256-row chunks); 2048^2 0.155 / 0.156 against 0.141 / 0.144 (128-row chunks).  Without
+// the staging the bands take 0.473 / 0.480 at 4096^2; 4-column bands 0.548 / 0.556 (their rows
+// are single 32-byte sectors); 16-column bands 0.464 / 0.474 at 7 CTAs per SM.  Bands run
+// wherever the shared-reciprocal quotients do; the chunk is the tallest of 256, 128 and 64 rows
+// that still makes kYWaves waves of CTAs.  Measured and dropped: the two shortcuts and an unrolled
+// row loop in the windows (more registers, more spills); tiles that recompute their 4 halo rows
+// instead of carrying them (0.489 ms at 4096^2 at best); an xi sweep that stores its result
+// transposed so the eta sweep can read contiguous lines (0.645 + 0.653 ms: the strided stores
+// cost more than the phases save); and the same cp.async staging in the xi sweep (0.3864 against
+// 0.3875 ms: its row loads are fully coalesced already).
 constexpr int kXT = 128;   // threads (and slots) of an xi-sweep CTA
 constexpr int kXMinBlocks = 8;
 constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA
@@ -36,10 +41,9 @@ constexpr int kYT = 128;   // columns of an eta-sweep window CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 24;    // rows of an eta-sweep strip
 constexpr int kBT = 128;   // threads of an eta-sweep band CTA
-constexpr int kBX = 4;     // columns of a band
+constexpr int kBX = 8;     // columns of a band
 constexpr int kBMinBlocks = 8;
-constexpr int kBChunk = 256;  // rows of a band CTA
-constexpr int kYWaves = 4;
+constexpr int kYWaves = 3;
 
 // A CTA sweeps R consecutive rows of one segment (blockIdx.y*R ..), strided by gridDim.y*R
 // when the grid has more rows than one launch's blocks cover.
@@ -66,13 +70,14 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
 }
 
 template <int LIM, bool SO, int MK>
-__global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g) {
-  __shared__ YBSmem<kBT, kBX> S;
+__global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g, int chunk) {
+  __shared__ YBSmem<kBT, kBX, true> S;
   if (g.ctl->done || !eta_valid(g)) return;
   double smax = 0.0;
   int bad = 0;
-  const int j0 = 1 + blockIdx.y * kBChunk;
-  ysweep_band<kBT, kBX, LIM, SO, MK, kOptFastDiv>(g, -1 + blockIdx.x * kBX, j0, j0 + kBChunk - 1, S, smax, bad);
+  const int j0 = 1 + blockIdx.y * chunk;
+  ysweep_band<kBT, kBX, LIM, SO, MK, kOptFastDiv, true>(g, -1 + blockIdx.x * kBX, j0, j0 + chunk - 1, S, smax,
+                                                        bad);
   block_max_to<kBT>(&g.ctl->smax_y, smax, S.red);
   if (bad) atomicOr(&g.ctl->status, bad);
 }
@@ -99,14 +104,24 @@ int sm_count() {
   }
   return n;
 }
+}  // namespace
+
+// The eta shape the launcher runs for g (kEtaWindow or kEtaBand).
+int eta_shape_of(const GridDev& g) {
+  if (!fast_div_ok(g)) return kEtaWindow;
+  return g.eta_shape == kEtaWindow ? kEtaWindow : kEtaBand;
+}
+
+namespace {
 template <int LIM, bool SO, int MK>
 void launch_y_t(const GridDev& g, cudaStream_t st) {
   dim3 gy((g.mx + kYT - 1) / kYT, (g.my + kYS - 1) / kYS);
-  const bool band = g.eta_shape == kEtaBand ||
-                    (g.eta_shape == kEtaAuto && (long long)gy.x * gy.y < (long long)kYWaves * kYMinBlocks * sm_count());
-  if (band && fast_div_ok(g)) {
-    dim3 gb((g.mx + 2 + kBX - 1) / kBX, (g.my + kBChunk - 1) / kBChunk);
-    yband_fp64_kernel<LIM, SO, MK><<<gb, kBT, 0, st>>>(g);
+  if (eta_shape_of(g) == kEtaBand) {
+    const long long bands = (g.mx + 2 + kBX - 1) / kBX, want = (long long)kYWaves * kBMinBlocks * sm_count();
+    int chunk = 256;
+    while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
+    dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
+    yband_fp64_kernel<LIM, SO, MK><<<gb, kBT, 0, st>>>(g, chunk);
   } else {
     ysweep_fp64_kernel<kYT, kYS, LIM, SO, MK><<<gy, kYT, 0, st>>>(g);
   }

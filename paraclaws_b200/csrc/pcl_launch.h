@@ -24,6 +24,8 @@ void launch_xsweep_gen(const GridDev& g, cudaStream_t st);
 void launch_ysweep_gen(const GridDev& g, cudaStream_t st);
 void launch_xsweep_fp64(const GridDev& g, cudaStream_t st);
 void launch_ysweep_fp64(const GridDev& g, cudaStream_t st);
+// the eta-sweep shape the specialised FP64 launcher runs for g (kEtaWindow or kEtaBand)
+int eta_shape_of(const GridDev& g);
 void launch_timectl(const GridDev& g, int op, int arg, double value, cudaStream_t st);
 void launch_ghost(const GridDev& g, int force, cudaStream_t st);
 void launch_upload(const GridDev& g, const double* staging_aos, cudaStream_t st);

@@ -49,6 +49,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// 8-byte asynchronous copy global -> shared (cp.async, sm_80+), in the calling thread's current
+// group; cp_async_commit closes the group, cp_async_wait<n> returns once at most n of the
+// thread's groups are still in flight, and the data of the others is visible to it.  The copies
+// read global memory only: they complete without any other thread's help.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Bounded wait for the phase with the given parity; false if it did not complete.
 // try_wait already suspends for a hardware-defined interval per probe, so the bound is
 // about a second of wall time at the default probe length.

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "pcl_fp64.cuh"
+#include "pcl_sm100.cuh"
 
 namespace pcl {
 
@@ -375,8 +376,15 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
 // start at row j0).  The caller checks the xi-sweep validity (eta_valid) and reduces smax and
 // the status bits over the CTA.
 // ------------------------------------------------------------------------------------------
-template <int NT, int TX>
-struct YBSmem {
+template <int NT, bool PF>
+struct YBStage {
+  double stg[2][3][NT];  // the cells of the next step, staged by cp.async while this one runs
+};
+template <int NT>
+struct YBStage<NT, false> {};
+
+template <int NT, int TX, bool PF = false>
+struct YBSmem : YBStage<NT, PF> {
   static constexpr int L = NT / TX;
   double sq[3][(L + 2) * TX], sf[3][(L + 2) * TX], ss[(L + 2) * TX], sk[(L + 2) * TX], slr[(L + 2) * TX];
   double sw1[3][(L + 2) * TX], sw2[3][(L + 2) * TX], ss2[(L + 2) * TX];
@@ -385,8 +393,10 @@ struct YBSmem {
   bool sok[(L + 2) * TX];
 };
 
-template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
-__device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1, YBSmem<NT, TX>& S,
+// PF: each thread stages its cell of the next step into shared memory (cp.async) before the
+// phases of this step, so the global loads overlap the four phases instead of opening them.
+template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0, bool PF = false>
+__device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1, YBSmem<NT, TX, PF>& S,
                                             double& smax_acc, int& bad_acc) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   constexpr int L = NT / TX;
@@ -410,15 +420,44 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
   double smax = 0.0;
   int bad = 0;
   const int jlast = min(j1, my);
+  // cell j = s + r of this thread's column into staging buffer b (rows past m_eta+2: nothing)
+  auto stage = [&](int s_, int b_) {
+    if constexpr (PF) {
+      const int j = s_ + r;
+      if (j <= my + 2) {
+        const double* src = (j >= 1 && j <= my) ? xsw : pre;
+        const long long o = (long long)(j + 1) * P + (ic + 1);
+        cp_async8(&S.stg[b_][0][t], src + o);
+        cp_async8(&S.stg[b_][1][t], src + o + g.plane);
+        cp_async8(&S.stg[b_][2][t], src + o + 2 * g.plane);
+      }
+      cp_async_commit();
+    }
+  };
+  if constexpr (PF) stage(j0 - 2, 0);
 
-  for (int s = j0 - 2; s - 2 <= jlast; s += L) {
+  int sb = 0;  // PF: staging buffer of this step
+  for (int s = j0 - 2; s - 2 <= jlast; s += L, sb ^= 1) {
+    if constexpr (PF) {
+      if (s + L - 2 <= jlast) {  // there is a next step: stage it, then wait for this one only
+        stage(s + L, sb ^ 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+    }
     {  // phase A: cell j = s + r into slot (r+2)TX + c
       const int j = s + r;
       const int sl = (r + 2) * TX + cx;
       if (j <= my + 2) {
         const double* src = (j >= 1 && j <= my) ? xsw : pre;
         const long long o = (long long)(j + 1) * P + (ic + 1);
-        const double h = src[o], hu = src[o + g.plane], hv = src[o + 2 * g.plane];
+        double h, hu, hv;
+        if constexpr (PF) {
+          h = S.stg[sb][0][t], hu = S.stg[sb][1][t], hv = S.stg[sb][2][t];
+        } else {
+          h = src[o], hu = src[o + g.plane], hv = src[o + 2 * g.plane];
+        }
         int cb = 0;
         const CellFlux F = cell_flux<1, OPT>(h, hu, hv, g.grav, &cb);
         if (j <= my + 1 && active) bad |= cb;

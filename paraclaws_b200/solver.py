@@ -215,6 +215,12 @@ class Solver:
         """Shape of the FP64 eta sweep (_lib.PCL_SHAPE_*): a schedule, the results stay the same."""
         _lib.check(self.L.pcl_set_sweep_shape(self.h, int(eta_shape)), "pcl_set_sweep_shape")
 
+    def sweep_shape(self) -> int:
+        """The eta-sweep shape the FP64 path runs for this grid (_lib.PCL_SHAPE_WINDOW or _BAND)."""
+        v = C.c_int()
+        _lib.check(self.L.pcl_get_sweep_shape(self.h, C.byref(v)), "pcl_get_sweep_shape")
+        return v.value
+
     def set_source_hook(self, fn_address: Optional[int], user: Optional[int] = None) -> None:
         """Install a pcl_source_fn (integrate_source_term with a non-zero phi); None: phi = 0."""
         _lib.check(self.L.pcl_set_source_hook(self.h, fn_address, user), "pcl_set_source_hook")
