@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
 
 template <int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g, int chunk) {
-  __shared__ YBSmem<kBT, kBX, true> S;
+  __shared__ YBSmem<kBT, kBX, true, MK == kMetricMapped> S;
   if (g.ctl->done || !eta_valid(g)) return;
   double smax = 0.0;
   int bad = 0;

@@ -382,11 +382,19 @@ struct YBStage {
 };
 template <int NT>
 struct YBStage<NT, false> {};
+template <int SLOTS, bool MP>
+struct YBMapped {
+  double slr[SLOTS];  // mapped grids: length ratio of the eta face below the cell
+};
+template <int SLOTS>
+struct YBMapped<SLOTS, false> {};
 
-template <int NT, int TX, bool PF = false>
-struct YBSmem : YBStage<NT, PF> {
+// PF: staging of the next step's cells; MP: mapped-grid metrics (the batch and uniform grids
+// leave both out when they do not use them, for shared memory).
+template <int NT, int TX, bool PF = false, bool MP = true>
+struct YBSmem : YBStage<NT, PF>, YBMapped<(NT / TX + 2) * TX, MP> {
   static constexpr int L = NT / TX;
-  double sq[3][(L + 2) * TX], sf[3][(L + 2) * TX], ss[(L + 2) * TX], sk[(L + 2) * TX], slr[(L + 2) * TX];
+  double sq[3][(L + 2) * TX], sf[3][(L + 2) * TX], ss[(L + 2) * TX], sk[(L + 2) * TX];
   double sw1[3][(L + 2) * TX], sw2[3][(L + 2) * TX], ss2[(L + 2) * TX];
   double sft[3][(L + 1) * TX];
   double red[NT / 32];
@@ -396,8 +404,9 @@ struct YBSmem : YBStage<NT, PF> {
 // PF: each thread stages its cell of the next step into shared memory (cp.async) before the
 // phases of this step, so the global loads overlap the four phases instead of opening them.
 template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0, bool PF = false>
-__device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1, YBSmem<NT, TX, PF>& S,
-                                            double& smax_acc, int& bad_acc) {
+__device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1,
+                                            YBSmem<NT, TX, PF, MK == kMetricMapped>& S, double& smax_acc,
+                                            int& bad_acc) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   constexpr int L = NT / TX;
   static_assert(NT % 32 == 0 && TX <= 16 && L >= 4, "band shape: rows 0, 1 within warp 0");
@@ -536,8 +545,8 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
       const int j = s - 2 + r;
       if (active && j >= j0 && j <= jlast) {
         const int c = r * TX + cx;
-        const double gl = MP ? S.slr[c] : gam;
-        const double gr = MP ? S.slr[c + TX] : gam;
+        double gl = gam, gr = gam;  // faces below and above the cell
+        if constexpr (MP) gl = S.slr[c], gr = S.slr[c + TX];
         const double dtk = UM ? dtod : dtod / S.sk[c];
         const double sp = S.ss2[c];
         const double sm = -S.ss2[c + TX];
