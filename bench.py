@@ -471,10 +471,10 @@ def batch_instances(n: int = 512, seed: int = 2):
     return sides, [ic.seeded_dam_params(k, offset=0.25) for k in range(n)]
 
 
-def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None, time_finals=None):
-    """One batch of the C4 instances, each stopping after `accepted_steps` accepted steps (0: at
-    its time_final, from `time_finals`, else never).  With perturb_seed, the FP64 start has h
-    raised by one ulp in 1% of the cells (host-built state)."""
+def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None):
+    """One batch of the C4 instances, each stopping after `accepted_steps` accepted steps (0:
+    never).  With perturb_seed, the FP64 start has h raised by one ulp in 1% of the cells
+    (host-built state)."""
     import numpy as np
 
     from paraclaws_b200 import control as ctl
@@ -482,18 +482,15 @@ def _make_batch(prec, sides, params, device, accepted_steps, perturb_seed=None, 
     from paraclaws_b200.batch import Batch
     b = Batch(len(sides), precision=prec, device=device)
     rng = np.random.Generator(np.random.PCG64(perturb_seed)) if perturb_seed is not None else None
-    for k, (m, p) in enumerate(zip(sides, params)):
+    for m, p in zip(sides, params):
         cu = ctl.CustomSettings(precision_mode=prec, dam_radius=p.radius, dam_h_in=p.h_in, dam_h_out=p.h_out,
                                 dam_x0=p.x0, dam_y0=p.y0, max_accepted_steps=accepted_steps)
-        tf = float(time_finals[k]) if time_finals is not None else 1.0e9
         q = None
         if rng is not None:
             q = ic.circular_dam(m, m, p.radius, p.h_in, p.h_out, p.x0, p.y0)
             mask = rng.random(q.shape[:2]) < 0.01
             q[..., 0] = np.where(mask, np.nextafter(q[..., 0], np.inf), q[..., 0])
-        # one snapshot time, the end: a clamp onto an intermediate snapshot time shortens a step by
-        # however close the run happens to be to it, and dt regrows only 1.2x per step after that
-        b.add(ctl.dam_break_control(m, limiter=1, bc=1, time_final=tf, number_of_snapshots=1), q, cu)
+        b.add(ctl.dam_break_control(m, limiter=1, bc=1, time_final=1.0e9), q, cu)
     return b
 
 
@@ -582,35 +579,40 @@ def form_batch(device, n=512, accepted_steps=200, precisions=("fp64", "mixed"), 
                                           "of_mixed_max_instance: the floor of the instance where mixed is "
                                           "furthest from FP64 (an instance that amplifies any perturbation "
                                           "shows it in both)"}
-        # The same comparison at the same physical time: after equal accepted-step counts the two
-        # runs can stand at different times (a near-tie of the largest wave speed between two cells
-        # resolved one step apart gives different dt sequences).  Each instance runs again in both
-        # precisions to the time its FP64 run reached, the last step clamped onto it (the FP64 run
-        # repeats its accepted steps exactly).
-        t_end = [finals["fp64"].stats(k).time for k in range(n)]
-        same = {}
-        for name, prec, pert in (("fp64", ctl.PRECISION_FP64, None), ("mixed", ctl.PRECISION_MIXED, None),
-                                 ("fp64_perturbed", ctl.PRECISION_FP64, 7)):
-            bb = _make_batch(prec, sides, params, device, 0, perturb_seed=pert, time_finals=t_end)
-            _run_to_completion(bb, torch)
-            same[name] = bb
-        l1_t, fl_t, dt_end = [], [], []
+        # Equal accepted-step counts put both precisions at the same physical time only where
+        # their dt sequences agree.  The time control keeps dt while CFL_target/CFL stays within
+        # 1% of 1 and rescales it once the ratio leaves that band; a CFL a rounding away from the
+        # band edge leaves it a step earlier in one precision, the dt sequences differ by ~1%
+        # from then on, and the states stand at different physical times (the sum of the dt each
+        # accepted step used).  So: L1(h) over the instances whose dt sequences agree to 1e-4
+        # relative -- above the 1e-6 the FP32 wave speeds round to, below a 1% rescale --
+        # (the arithmetic difference of the two precisions), and for the others the physical
+        # time offset beside their L1.  (Running both to one time_final does not help:
+        # the time control advances `time` by the next step's dt, so a run that reaches it one
+        # step later holds the state one full step further on.)
+        match, l1_match, off = [], [], []
         for k in range(n):
-            ref = same["fp64"].download(k)[2:-2, 2:-2, 0]
-            scale = float(np.abs(ref).sum())
-            l1_t.append(float(np.abs(same["mixed"].download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
-            fl_t.append(float(np.abs(same["fp64_perturbed"].download(k)[2:-2, 2:-2, 0] - ref).sum() / scale))
-            dt_end.append(abs(same["mixed"].stats(k).time - same["fp64"].stats(k).time))
-        for bb in same.values():
-            bb.close()
-        worst_t = int(np.argmax(l1_t))
-        res["l1_h_mixed_vs_fp64_same_time"] = {
-            "median": float(np.median(l1_t)), "p99": float(np.percentile(l1_t, 99)), "max": float(max(l1_t)),
-            "max_instance": worst_t, "max_instance_side": int(sides[worst_t]),
-            "instances_le_1e-5": int(sum(v <= 1e-5 for v in l1_t)),
-            "fp64_floor_median": float(np.median(fl_t)), "fp64_floor_max": float(max(fl_t)),
-            "end_time_diff_max": float(max(dt_end)),
-            "note": "both precisions run to the time the FP64 instance reached after the accepted steps"}
+            a64, amx = finals["fp64"].step_log(k), finals["mixed"].step_log(k)
+            same_len = len(a64.dt) == len(amx.dt)
+            rel = float(np.max(np.abs(amx.dt - a64.dt) / a64.dt)) if same_len and len(a64.dt) else float("inf")
+            tp64 = float(a64.dt[a64.ierr > 0].sum())
+            tpmx = float(amx.dt[amx.ierr > 0].sum())
+            if rel <= 1e-4:
+                match.append(k)
+                l1_match.append(l1_mixed[k])
+            else:
+                off.append({"instance": k, "side": int(sides[k]), "l1_h": l1_mixed[k],
+                            "dt_rel_diff_max": rel, "physical_time_offset_rel": abs(tpmx - tp64) / tp64})
+        off.sort(key=lambda e: -e["l1_h"])
+        res["l1_h_mixed_vs_fp64_dt_matched"] = {
+            "instances": len(match), "median": float(np.median(l1_match)) if l1_match else None,
+            "p99": float(np.percentile(l1_match, 99)) if l1_match else None,
+            "max": float(max(l1_match)) if l1_match else None,
+            "instances_le_1e-5": int(sum(v <= 1e-5 for v in l1_match)),
+            "dt_diverged": off[:8], "dt_diverged_count": len(off),
+            "note": "instances whose mixed dt sequence equals the FP64 one to 1e-4 relative over all "
+                    "attempts (no dt rescale one step apart), so both states stand at the same "
+                    "physical time to that accuracy"}
     for b in finals.values():
         b.close()
     res["instances"] = n
@@ -687,7 +689,7 @@ def target_summary(fp64_value: float, forms: dict) -> dict:
     mx = b.get("mixed", {})
     l1 = b.get("l1_h_mixed_vs_fp64", {})
     fl = b.get("l1_h_fp64_floor", {})
-    lt = b.get("l1_h_mixed_vs_fp64_same_time", {})
+    lt = b.get("l1_h_mixed_vs_fp64_dt_matched", {})
     srv = forms.get("serving", {})
 
     def serve(name, rate):
@@ -705,14 +707,14 @@ def target_summary(fp64_value: float, forms: dict) -> dict:
          "l1_h_fp64_floor_median": _sig(fl.get("median")),
          "l1_h_le_1e-5_instances": l1.get("instances_le_1e-5"),
          "l1_h_fp64_floor_of_max_instance": _sig(fl.get("of_mixed_max_instance")),
-         "l1_h_same_time_median": _sig(lt.get("median")), "l1_h_same_time_max": _sig(lt.get("max")),
-         "l1_h_same_time_le_1e-5_instances": lt.get("instances_le_1e-5"),
+         "l1_h_dt_matched_max": _sig(lt.get("max")), "dt_matched_instances": lt.get("instances"),
+         "dt_diverged_instances": lt.get("dt_diverged_count"),
          "serving_mixed": serve("mixed", 12.0), "serving_fp64": serve("fp64", 3.0),
          "workload": "C4, 512 instances x 200 accepted steps; serving C5"}
     if v:
         t["met"] = {"speedup_ge_2": v / fp64_value >= 2.0, "effective_roofline_ge_0.70": mx["effective_roofline_frac"] >= 0.7,
                     "l1_h_max_le_1e-5": bool(l1) and l1["max"] <= 1e-5,
-                    "l1_h_same_time_max_le_1e-5": bool(lt) and lt["max"] <= 1e-5}
+                    "l1_h_dt_matched_max_le_1e-5": bool(lt) and lt.get("max") is not None and lt["max"] <= 1e-5}
     return t
 
 
