@@ -3,7 +3,7 @@
 // the wave-speed reduction and the time control in FP64.
 //
 // Work item: a strip of TXI = 124 columns x a segment of TY rows.  The CTA streams the rows
-// j0-2 .. j1+2 of its strip (plus two halo columns each side) through a four-slot shared-memory
+// j0-2 .. j1+2 of its strip (plus two halo columns each side) through a five-slot shared-memory
 // ring filled by bulk copies (cp.async.bulk, completion on an mbarrier), three rows ahead.  For each
 // row: the xi sweep of that row runs in shared memory (per-cell flux data, HLL per interface,
 // limited correction flux, update); thread t keeps the x-swept FP64 value of its own column
@@ -33,8 +33,12 @@ namespace mixed {
 
 constexpr int NT = 128;      // threads per CTA = slots of a streamed row
 constexpr int TXI = NT - 4;  // interior columns of a strip
-constexpr int RING = 4;      // row slots
+// Row slots: the copy issued at the start of row k refills the slot of row k+AHEAD-RING = k-2,
+// which every thread finished before it passed row k-1's copy-wait vote, so a row needs no
+// barrier after its last read of the ring.
+constexpr int RING = 5;
 constexpr int AHEAD = 3;     // rows in flight ahead of the one being processed
+static_assert(RING >= AHEAD + 2, "the refilled slot must be two rows old");
 constexpr float kEps = 1e-10f;
 
 struct CellM {
@@ -197,7 +201,7 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
       for (int p = 0; p < 3; ++p) bulk_g2s(&S.ring[slot][p][0], src + p * PL, ncopy * 8u, &S.bar[slot]);
     }
   };
-  for (int k = 0; k < AHEAD && k < nrows; ++k) issue(jfirst + k, (base + k) & (RING - 1));
+  for (int k = 0; k < AHEAD && k < nrows; ++k) issue(jfirst + k, (base + k) % RING);
 
   int bad = 0;
   float smx = 0.f, smy = 0.f;
@@ -220,9 +224,9 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
   for (int k = 0; k < nrows; ++k) {
     const int jr = jfirst + k;
     const unsigned kk = base + k;
-    const int slot = kk & (RING - 1);
+    const int slot = kk % RING;
     if (k + AHEAD < nrows) {
-      issue(jr + AHEAD, (kk + AHEAD) & (RING - 1));
+      issue(jr + AHEAD, (kk + AHEAD) % RING);
       issued++;
     }
     const bool ok = INJ ? mbar_wait_bounded(&S.bar[slot], (kk / RING) & 1u, probes)
@@ -335,16 +339,15 @@ __device__ __forceinline__ bool mixed_item(const G& g, int strip, int seg, int T
       }
       cprev = cn;
     }
-    __syncthreads();  // this row's slot is refilled at the start of the next row
   }
 
   if (timed_out && t == 0) {
     // drain the copies this CTA still has in flight before its shared memory goes away
     for (int k = consumed; k < issued; ++k) {
       if (INJ)
-        mbar_wait_bounded(&S.bar[(base + k) & (RING - 1)], ((base + k) / RING) & 1u, probes);
+        mbar_wait_bounded(&S.bar[(base + k) % RING], ((base + k) / RING) & 1u, probes);
       else
-        mbar_wait_bounded(&S.bar[(base + k) & (RING - 1)], ((base + k) / RING) & 1u);
+        mbar_wait_bounded(&S.bar[(base + k) % RING], ((base + k) / RING) & 1u);
     }
   }
   rows = base + issued;
