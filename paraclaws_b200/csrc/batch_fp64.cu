@@ -40,10 +40,8 @@ __device__ __forceinline__ void run_item(const GridDev& g, int kind, int a, int 
   int bad = 0;
   if (kind == kItemX) {
     const int jend = min(a + v.x_rows - 1, g.my);
-    for (int j = a; j <= jend; ++j) {
-      xsweep_segment<kThreads, LIM, SO, MK, OPT>(g, j, b, S.x, smax, bad);
-      __syncthreads();  // the segment's shared arrays are reused by the next row
-    }
+    for (int j = a, par = 0; j <= jend; ++j, par ^= 1)
+      xsweep_segment<kThreads, LIM, SO, MK, OPT>(g, j, b, S.x, smax, bad, par);
     xsweep_finish<kThreads>(g, smax, bad, S.x);
   } else {
     if (!eta_valid(g)) return;  // the same answer for every thread: all xi items are done

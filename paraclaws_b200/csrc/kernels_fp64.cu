@@ -53,12 +53,11 @@ __global__ void __launch_bounds__(NT, kXMinBlocks) xsweep_fp64_kernel(GridDev g)
   if (g.ctl->done) return;
   double smax = 0.0;
   int bad = 0;
+  int par = 0;
   for (int jb = 1 + blockIdx.y * R; jb <= g.my; jb += gridDim.y * R) {
     const int je = min(jb + R - 1, g.my);
-    for (int j = jb; j <= je; ++j) {
-      xsweep_segment<NT, LIM, SO, MK, OPT>(g, j, 1 + blockIdx.x * (NT - 4), S, smax, bad);
-      __syncthreads();  // the shared arrays are reused by the next row
-    }
+    for (int j = jb; j <= je; ++j, par ^= 1)
+      xsweep_segment<NT, LIM, SO, MK, OPT>(g, j, 1 + blockIdx.x * (NT - 4), S, smax, bad, par);
   }
   xsweep_finish<NT>(g, smax, bad, S);
 }

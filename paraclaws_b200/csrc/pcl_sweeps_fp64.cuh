@@ -43,7 +43,9 @@ __device__ __forceinline__ void block_max_to(unsigned long long* dst, double v, 
 // Shared memory of one xi-sweep segment (per-slot cell data, waves, correction flux).
 template <int NT>
 struct XSmem {
-  double sq[3][NT], sf[3][NT], ss[NT], sk[NT];
+  // sq and sk in two copies by row parity: phase D of a row reads them after its last barrier,
+  // while phase A of the next row writes them, so consecutive rows need no barrier between them
+  double sq[2][3][NT], sf[3][NT], ss[NT], sk[2][NT];
   double sw1[3][NT], sw2[3][NT], ss2[NT], sft[3][NT];
   double red[NT / 32];
   bool sok[NT];  // kOptFastDiv: the cell is in the range of the shared-reciprocal quotients
@@ -60,9 +62,12 @@ __device__ __forceinline__ void xsweep_finish(const GridDev& g, double smax, int
 // mask of pcl_fp64.cuh (same results for every value).  The row's wave-speed maximum is
 // folded into smax_acc and its status bits into bad_acc; the caller reduces them over the CTA
 // once for all the rows it sweeps (xsweep_finish).
+// Rows swept one after another alternate `par` (0, 1, 0, ...) and need no barrier between them:
+// every shared array phase D reads is either in the row's own parity copy or written by the next
+// row only after that row's first barrier.
 template <int NT, int LIM, bool SO, int MK = kMetricTable, int OPT = 0>
 __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, XSmem<NT>& S, double& smax_acc,
-                                               int& bad_acc) {
+                                               int& bad_acc, int par = 0) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   const Ctl* ctl = g.ctl;
   constexpr int L = NT - 4;
@@ -75,10 +80,10 @@ __device__ __forceinline__ void xsweep_segment(const GridDev& g, int j, int i0, 
   const double* q1 = q0 + g.plane;
   const double* q2 = q1 + g.plane;
 
-  auto& sq = S.sq;
+  auto& sq = S.sq[par];
   auto& sf = S.sf;
   auto& ss = S.ss;
-  auto& sk = S.sk;
+  auto& sk = S.sk[par];
   auto& sw1 = S.sw1;
   auto& sw2 = S.sw2;
   auto& ss2 = S.ss2;
