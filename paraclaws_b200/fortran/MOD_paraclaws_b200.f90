@@ -97,6 +97,19 @@ module MOD_paraclaws_b200
             integer(c_int), value :: nparams
         end function
 
+        ! schedule of the FP64 eta sweep (PCL_SHAPE_AUTO 0, _WINDOW 1, _BAND 2); results unchanged
+        integer(c_int) function pcl_set_sweep_shape(ctx, eta_shape) bind(C)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: eta_shape
+        end function
+
+        integer(c_int) function pcl_get_sweep_shape(ctx, eta_shape) bind(C)
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+            integer(c_int), intent(out) :: eta_shape
+        end function
+
         integer(c_int) function pcl_update_rank_boundaries(ctx) bind(C)
             import :: c_int, c_ptr
             type(c_ptr), value :: ctx
