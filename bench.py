@@ -682,7 +682,7 @@ def _sig(x, digits=4):
 
 
 def target_summary(fp64_value: float, forms: dict) -> dict:
-    """The north-star target, compact: the mixed-precision batched form (C4, accepted-step work)
+    """The target, compact: the mixed-precision batched form (C4, accepted-step work)
     against the plain FP64 path (this line's value), its roofline fractions, its L1(h) against
     the FP64 batch, and the serving latencies of both precisions."""
     b = forms.get("batch", {})
