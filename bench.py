@@ -878,7 +878,7 @@ def run_ours(args) -> None:
                  "serving": form_serving(local),
                  "precision": form_precision(local)}
         line["forms"] = forms
-        # last key of the line: the north-star target on its own stated terms
+        # last key of the line: the target on its own stated terms
         line["target"] = target_summary(value, forms)
     s.close()
     if dist is not None:
