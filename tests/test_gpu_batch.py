@@ -237,3 +237,33 @@ def test_autotuner_picks_a_schedule(pcl, tmp_path):
     best2, _ = autotune(b, cache=tmp_path / "t.json")
     assert best2 == best
     b.close()
+
+
+@pytest.mark.parametrize("schedule", [Schedule(x_rows=8, y_rows=64), Schedule(x_rows=1, y_rows=4, blocks_per_sm=1)])
+def test_large_and_small_grids_match_alone(pcl, schedule):
+    """FP64 grids of more than 512^2 cells beside small ones in the same launches.  m_xi = 519
+    leaves the last 4-column eta band one cell wide (its ghost side falls to the finishing CTA);
+    517 does not.  Both schedules (few long items with edge-item ghost fill, many short ones with
+    the finishing CTA's) end bit-identical to each grid run alone, ghost cells included."""
+    shapes = [(519, 520), (517, 513), (100, 64), (260, 33)]
+    codes = [(1, 3, 2, 3), (3, 1, 3, 2), (2, 2, 1, 1), (1, 1, 1, 1)]
+    cases = []
+    for k, ((mx, my), (b0, b1, b2, b3)) in enumerate(zip(shapes, codes)):
+        c = dataclasses.replace(ctl.dam_break_control(mx, limiter=1 + k % 4, bc=1, time_final=0.01), m_eta=my,
+                                bc_xi_lower=b0, bc_xi_upper=b1, bc_eta_lower=b2, bc_eta_upper=b3)
+        p = ic.seeded_dam_params(k + 40, offset=0.25)
+        cases.append((c, ic.circular_dam(mx, my, p.radius, p.h_in, p.h_out, p.x0, p.y0)))
+    b = Batch(4, precision=ctl.PRECISION_FP64)
+    b.set_schedule(schedule)
+    slots = [b.add(c, q) for c, q in cases]
+    for _ in range(400):
+        b.step(16)
+        done, status = b.poll()
+        assert all(status[s] == 0 for s in slots)
+        if all(done[s] == 1 for s in slots):
+            break
+    for s, (c, q) in zip(slots, cases):
+        qa, la = _alone(c, q, ctl.PRECISION_FP64)
+        assert np.array_equal(b.step_log(s).dt, la.dt)
+        assert np.array_equal(b.download(s), qa)
+    b.close()
