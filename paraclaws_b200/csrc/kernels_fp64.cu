@@ -5,6 +5,8 @@
 // pcl_sweeps_fp64.cuh.  Built with --fmad=false.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "pcl_launch.h"
 #include "pcl_sweeps_fp64.cuh"
 
@@ -21,12 +23,15 @@ namespace {
 // per SM (4 rows: 0.397; the limiter shortcut on top: 0.399).
 // The eta sweep has two shapes.  Column windows (ysweep_strip) at 6 CTAs of 128 threads per SM
 // (80 registers, a few spilled window values) with 24-row strips (16 rows: +1%, 32: +1%).  Bands
-// of 8 columns (ysweep_band) at 8 CTAs per SM (64 registers, no spills), each thread staging its
-// cell of the next 16-row step by cp.async while the phases of this one run.  Eta sweep in ms
-// on bumps after 8 / 200 steps, windows against bands: 4096^2 0.482 / 0.499 against 0.465 /
-// 0.468 (256-row chunks); 2048^2 0.155 / 0.156 against 0.141 / 0.144 (128-row chunks).  Without
-// the staging the bands take 0.473 / 0.480 at 4096^2; 4-column bands 0.548 / 0.556 (their rows
-// are single 32-byte sectors); 16-column bands 0.464 / 0.474 at 7 CTAs per SM.  Bands run
+// (ysweep_band), 64 registers, no spills, each thread staging its cell of the next step by
+// cp.async while the phases of this one run: 16 columns x 16 rows per step in 256-thread CTAs,
+// 4 per SM (55 KB of shared memory each), a barrier per 256 cells.  Against 8 columns x 16 rows
+// in 128-thread CTAs, 8 per SM (the lab figures below): eta sweep 0.460 against 0.465 ms at
+// 4096^2, whole step 3.13 against 3.15 ms at 8192^2; 8 columns x 32 rows in 256 threads: 0.503
+// ms.  Lab, eta sweep in ms on bumps after 8 / 200 steps, windows against 8-column bands: 4096^2
+// 0.482 / 0.499 against 0.465 / 0.468 (256-row chunks); 2048^2 0.155 / 0.156 against 0.141 /
+// 0.144 (128-row chunks).  Without the staging the bands take 0.473 / 0.480 at 4096^2; 4-column
+// bands 0.548 / 0.556 (their rows are single 32-byte sectors).  Bands run
 // wherever the shared-reciprocal quotients do; the chunk is the tallest of 256, 128 and 64 rows
 // that still makes kYWaves waves of CTAs.  Measured and dropped: the two shortcuts and an unrolled
 // row loop in the windows (more registers, more spills); tiles that recompute their 4 halo rows
@@ -40,9 +45,9 @@ constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA
 constexpr int kYT = 128;   // columns of an eta-sweep window CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 24;    // rows of an eta-sweep strip
-constexpr int kBT = 128;   // threads of an eta-sweep band CTA
-constexpr int kBX = 8;     // columns of a band
-constexpr int kBMinBlocks = 8;
+constexpr int kBT = 256;   // threads of an eta-sweep band CTA
+constexpr int kBX = 16;    // columns of a band
+constexpr int kBMinBlocks = 4;
 constexpr int kYWaves = 3;
 
 // A CTA sweeps R consecutive rows of one segment (blockIdx.y*R ..), strided by gridDim.y*R
@@ -70,7 +75,8 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
 
 template <int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g, int chunk) {
-  __shared__ YBSmem<kBT, kBX, true, MK == kMetricMapped> S;
+  extern __shared__ __align__(16) unsigned char band_smem[];
+  auto& S = *reinterpret_cast<YBSmem<kBT, kBX, true, MK == kMetricMapped>*>(band_smem);
   if (g.ctl->done || !eta_valid(g)) return;
   double smax = 0.0;
   int bad = 0;
@@ -120,7 +126,17 @@ void launch_y_t(const GridDev& g, cudaStream_t st) {
     int chunk = 256;
     while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
     dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
-    yband_fp64_kernel<LIM, SO, MK><<<gb, kBT, 0, st>>>(g, chunk);
+    // 55 KB of dynamic shared memory: allowed once per device for each build of the kernel
+    constexpr int smem = (int)sizeof(YBSmem<kBT, kBX, true, MK == kMetricMapped>);
+    static std::atomic<unsigned long long> allowed{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(allowed.load() & bit)) {
+      cudaFuncSetAttribute(yband_fp64_kernel<LIM, SO, MK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      allowed.fetch_or(bit);
+    }
+    yband_fp64_kernel<LIM, SO, MK><<<gb, kBT, smem, st>>>(g, chunk);
   } else {
     ysweep_fp64_kernel<kYT, kYS, LIM, SO, MK><<<gy, kYT, 0, st>>>(g);
   }
