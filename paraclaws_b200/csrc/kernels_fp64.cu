@@ -19,26 +19,27 @@ namespace {
 // Launch shapes (measured on B200, bumps after 100-300 steps, minmod; every variant
 // bit-identical): the xi sweep at 8 CTAs of 128 threads per SM, each CTA sweeping 8 rows of its
 // segment with one block reduction at the end, with the shared-reciprocal quotients
-// (kOptFastDiv): 0.391 ms at 4096^2 against 0.508 ms for one row per 256-thread CTA at 5 CTAs
-// per SM (4 rows: 0.397; the limiter shortcut on top: 0.399).
+// (kOptFastDiv) and the row parity buffers: 0.387 ms at 4096^2 against 0.508 ms for one row per
+// 256-thread CTA at 5 CTAs per SM (4 rows: 0.397; the limiter shortcut on top: 0.399; 8 rows in
+// 256-thread CTAs with 252-cell segments, 4 per SM: 0.415).
 // The eta sweep has two shapes.  Column windows (ysweep_strip) at 6 CTAs of 128 threads per SM
 // (80 registers, a few spilled window values) with 24-row strips (16 rows: +1%, 32: +1%).  Bands
 // (ysweep_band), 64 registers, no spills, each thread staging its cell of the next step by
 // cp.async while the phases of this one run: 16 columns x 16 rows per step in 256-thread CTAs,
 // 4 per SM (55 KB of shared memory each), a barrier per 256 cells.  Against 8 columns x 16 rows
-// in 128-thread CTAs, 8 per SM (the lab figures below): eta sweep 0.460 against 0.465 ms at
-// 4096^2, whole step 3.13 against 3.15 ms at 8192^2; 8 columns x 32 rows in 256 threads: 0.503
-// ms.  Lab, eta sweep in ms on bumps after 8 / 200 steps, windows against 8-column bands: 4096^2
-// 0.482 / 0.499 against 0.465 / 0.468 (256-row chunks); 2048^2 0.155 / 0.156 against 0.141 /
-// 0.144 (128-row chunks).  Without the staging the bands take 0.473 / 0.480 at 4096^2; 4-column
-// bands 0.548 / 0.556 (their rows are single 32-byte sectors).  Bands run
-// wherever the shared-reciprocal quotients do; the chunk is the tallest of 256, 128 and 64 rows
-// that still makes kYWaves waves of CTAs.  Measured and dropped: the two shortcuts and an unrolled
-// row loop in the windows (more registers, more spills); tiles that recompute their 4 halo rows
-// instead of carrying them (0.489 ms at 4096^2 at best); an xi sweep that stores its result
-// transposed so the eta sweep can read contiguous lines (0.645 + 0.653 ms: the strided stores
-// cost more than the phases save); and the same cp.async staging in the xi sweep (0.3864 against
-// 0.3875 ms: its row loads are fully coalesced already).
+// in 128-thread CTAs, 8 per SM: eta sweep 0.460 against 0.465 ms at 4096^2, whole step 3.13
+// against 3.15 ms at 8192^2; 8 columns x 32 rows in 256 threads: 0.503 ms; 16 columns x 32 rows
+// in 512 threads (2 CTAs per SM): 0.521 ms.  Lab, eta sweep in ms on bumps after 8 / 200 steps,
+// windows against 8-column bands: 4096^2 0.482 / 0.499 against 0.465 / 0.468 (256-row chunks);
+// 2048^2 0.155 / 0.156 against 0.141 / 0.144 (128-row chunks).  Without the staging the bands
+// take 0.473 / 0.480 at 4096^2; 4-column bands 0.548 / 0.556 (their rows are single 32-byte
+// sectors).  Bands run wherever the shared-reciprocal quotients do; the chunk is the tallest of
+// 256, 128 and 64 rows that still makes kYWaves waves of CTAs.  Measured and dropped: the two
+// shortcuts and an unrolled row loop in the windows (more registers, more spills); tiles that
+// recompute their 4 halo rows instead of carrying them (0.489 ms at 4096^2 at best); an xi sweep
+// that stores its result transposed so the eta sweep can read contiguous lines (0.645 + 0.653
+// ms: the strided stores cost more than the phases save); and the same cp.async staging in the
+// xi sweep (0.3864 against 0.3875 ms: its row loads are fully coalesced already).
 constexpr int kXT = 128;   // threads (and slots) of an xi-sweep CTA
 constexpr int kXMinBlocks = 8;
 constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA
