@@ -194,9 +194,10 @@ int pcl_set_source_hook(pcl_ctx* ctx, pcl_source_fn fn, void* user);
 int pcl_set_equation(pcl_ctx* ctx, int module, const double* params, int nparams);
 
 /* Shape of the FP64 eta sweep, a schedule that never changes results.  PCL_SHAPE_AUTO (the
-   default) picks column windows when they fill the GPU with several waves of CTAs (large grids)
-   and 4-column bands below that; PCL_SHAPE_WINDOW and PCL_SHAPE_BAND force one (bands need g in
-   [2^-20, 2^20]; outside it the windows run).  Specialised shallow-water module only. */
+   default) and PCL_SHAPE_BAND run the bands (shared-memory phases along the columns of narrow
+   column bands); PCL_SHAPE_WINDOW runs column windows (one thread per column over a strip of
+   rows).  For the specialised shallow-water module the bands need g in [2^-20, 2^20]; outside
+   it the windows run.  Applies to every equation module's FP64 path. */
 #define PCL_SHAPE_AUTO 0
 #define PCL_SHAPE_WINDOW 1
 #define PCL_SHAPE_BAND 2

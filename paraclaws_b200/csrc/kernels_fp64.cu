@@ -114,7 +114,8 @@ int sm_count() {
 
 // The eta shape the launcher runs for g (kEtaWindow or kEtaBand).
 int eta_shape_of(const GridDev& g) {
-  if (!fast_div_ok(g)) return kEtaWindow;
+  // the generic modules' bands need no shared reciprocals (kernels_gen.cu)
+  if (g.eq == PCL_EQ_SHALLOW_WATER && !fast_div_ok(g)) return kEtaWindow;
   return g.eta_shape == kEtaWindow ? kEtaWindow : kEtaBand;
 }
 

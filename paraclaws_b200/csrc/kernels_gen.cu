@@ -11,8 +11,14 @@ namespace {
 
 constexpr int kGXT = 128;  // threads (slots) of an xi-sweep CTA
 constexpr int kGXRows = 4; // rows of one segment per xi-sweep CTA
-constexpr int kGYT = 128;  // columns of an eta-sweep CTA
+constexpr int kGYT = 128;  // columns of an eta-sweep window CTA
 constexpr int kGYS = 32;   // rows of an eta-sweep strip
+// Eta sweep in bands (the default; gen::ysweep_band): 128-thread CTAs on 8-column bands, 16 rows
+// per step, chunks of 256 rows halved to 128 or 64 while the grid makes fewer than 3 waves, 6 CTAs
+// per SM.  At 4096^2 the dam-break module runs at 10.7 G cell-updates/s against 9.1 G with the
+// column windows (5 CTAs per SM without the register cap: 10.4 G), acoustics 12.8 G either way.
+constexpr int kGBT = 128;
+constexpr int kGBX = 8;
 
 template <int N, int LIM, bool SO>
 __global__ void __launch_bounds__(kGXT) xsweep_gen_kernel(GridDev g) {
@@ -37,6 +43,29 @@ __global__ void __launch_bounds__(kGYT) ysweep_gen_kernel(GridDev g) {
 }
 
 template <int N, int LIM, bool SO>
+__global__ void __launch_bounds__(kGBT, 6) yband_gen_kernel(GridDev g, int chunk) {
+  __shared__ gen::YBSmem<kGBT, kGBX, N> S;
+  if (g.ctl->done || !eta_valid(g)) return;
+  double smax = 0.0;
+  int bad = 0;
+  const int j0 = 1 + blockIdx.y * chunk;
+  gen::ysweep_band<kGBT, kGBX, N, LIM, SO>(g, -1 + blockIdx.x * kGBX, j0, j0 + chunk - 1, S, smax, bad);
+  block_max_to<kGBT>(&g.ctl->smax_y, smax, S.red);
+  if (bad) atomicOr(&g.ctl->status, bad);
+}
+
+int sm_count_gen() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int N, int LIM, bool SO>
 struct GenLaunch {
   static void x(const GridDev& g, cudaStream_t st) {
     const int rb = (g.my + kGXRows - 1) / kGXRows;
@@ -44,8 +73,18 @@ struct GenLaunch {
     xsweep_gen_kernel<N, LIM, SO><<<gx, kGXT, 0, st>>>(g);
   }
   static void y(const GridDev& g, cudaStream_t st) {
-    dim3 gy((g.mx + kGYT - 1) / kGYT, (g.my + kGYS - 1) / kGYS);
-    ysweep_gen_kernel<N, LIM, SO><<<gy, kGYT, 0, st>>>(g);
+    if (g.eta_shape == kEtaWindow) {
+      dim3 gy((g.mx + kGYT - 1) / kGYT, (g.my + kGYS - 1) / kGYS);
+      ysweep_gen_kernel<N, LIM, SO><<<gy, kGYT, 0, st>>>(g);
+      return;
+    }
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, yband_gen_kernel<N, LIM, SO>, kGBT, 0);
+    const long long bands = (g.mx + 2 + kGBX - 1) / kGBX, want = 3LL * (occ > 0 ? occ : 1) * sm_count_gen();
+    int chunk = 256;
+    while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
+    dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
+    yband_gen_kernel<N, LIM, SO><<<gb, kGBT, 0, st>>>(g, chunk);
   }
 };
 

@@ -373,5 +373,203 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
   if (bad) atomicOr(&ctl->status, bad);
 }
 
+// ------------------------------------------------------------------------------------------
+// eta sweep in bands (pcl_sweeps_fp64.cuh: ysweep_band), N components: a CTA walks its chunk of
+// rows down a band of TX columns in steps of L = NT/TX rows, the four phases of the xi sweep
+// running along the columns, the last two cells, two interfaces and one correction flux of a
+// step carried into the next in history slots, and each thread's cell of the next step staged
+// by cp.async while the phases of this one run.  Slot (r, c) = row r of the step (+2 history
+// rows), column c of the band.  Same semantics as ysweep_strip; the caller checks the xi-sweep
+// validity and reduces smax and the status bits over the CTA.
+// ------------------------------------------------------------------------------------------
+template <int NT, int TX, int N>
+struct YBSmem {
+  static constexpr int L = NT / TX;
+  static constexpr int CS = (L + 2) * TX;
+  double sq[N][CS], sf[N][CS], ss[CS], sk[CS];
+  double sw1[N][CS], sw2[N][CS], ss2[CS];
+  double sft[N][(L + 1) * TX];
+  double stg[2][N][NT];
+  double red[NT / 32];
+};
+
+template <int NT, int TX, int N, int LIM, bool SO>
+__device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1, YBSmem<NT, TX, N>& S,
+                                            double& smax_acc, int& bad_acc) {
+  constexpr int L = NT / TX;
+  static_assert(NT % 32 == 0 && TX <= 16 && L >= 4, "band shape: rows 0, 1 within warp 0");
+  const Ctl* ctl = g.ctl;
+  const int cur = ctl->cur;
+  const int xb = cur == 2 ? 0 : cur + 1;
+  const int yb = cur == 0 ? 2 : cur - 1;
+  const double dtod = ctl->dtod_y;
+  const int mx = g.mx, my = g.my;
+  const long long P = g.pitch;
+  const int t = threadIdx.x;
+  const int cx = t % TX, r = t / TX;
+  const int i = i0 + cx;
+  const bool active = i >= 1 && i <= mx;
+  const int ic = i < 1 ? 1 : (i > mx ? mx : i);
+  const double* pre = buffer(g, cur);
+  const double* xsw = buffer(g, xb);
+  double* outp = buffer(g, yb);
+  const double gam = __ldg(g.colm + (ic + 1) * kColMetrics + 2);
+  double smax = 0.0;
+  int bad = 0;
+  const int jlast = min(j1, my);
+  auto stage = [&](int s_, int b_) {  // cell s_ + r of this thread's column (none past m_eta+2)
+    const int j = s_ + r;
+    if (j <= my + 2) {
+      const double* src = (j >= 1 && j <= my) ? xsw : pre;
+      const long long o = (long long)(j + 1) * P + (ic + 1);
+#pragma unroll
+      for (int me = 0; me < N; ++me) cp_async8(&S.stg[b_][me][t], src + o + me * g.plane);
+    }
+    cp_async_commit();
+  };
+  stage(j0 - 2, 0);
+
+  int sb = 0;
+  for (int s = j0 - 2; s - 2 <= jlast; s += L, sb ^= 1) {
+    if (s + L - 2 <= jlast) {
+      stage(s + L, sb ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    {  // phase A: cell j = s + r into slot (r+2)TX + c
+      const int j = s + r;
+      const int sl = (r + 2) * TX + cx;
+      if (j <= my + 2) {
+        double q[N];
+#pragma unroll
+        for (int me = 0; me < N; ++me) q[me] = S.stg[sb][me][t];
+        int cb = 0;
+        const Cell<N> F = cell_flux<N, 1>(g.eq, q, g.eqp, &cb);
+        if (j <= my + 1 && active) bad |= cb;  // getJakobi runs on rows -1 .. m_eta+1
+#pragma unroll
+        for (int me = 0; me < N; ++me) {
+          S.sq[me][sl] = q[me];
+          S.sf[me][sl] = F.f[me];
+        }
+        S.ss[sl] = F.s;
+        S.sk[sl] = capacity(g.rowm, g.colm, ic, j, g.area_scale);
+      }
+    }
+    __syncthreads();
+    {  // phase B: interface k = s + r (cells k-1, k) into slot (r+2)TX + c
+      const int k = s + r;
+      const int sl = (r + 2) * TX + cx, sm = sl - TX;
+      WavesN<N> W;
+      double s2 = 0.0;
+      if (k <= my + 1 && k >= j0 - 1) {
+        double qL[N], qR[N];
+        Cell<N> FL, FR;
+#pragma unroll
+        for (int me = 0; me < N; ++me) {
+          qL[me] = S.sq[me][sm];
+          qR[me] = S.sq[me][sl];
+          FL.f[me] = S.sf[me][sm];
+          FR.f[me] = S.sf[me][sl];
+        }
+        FL.s = S.ss[sm];
+        FR.s = S.ss[sl];
+        s2 = hll<N>(qL, FL, qR, FR, W);
+        if (active) smax = fmax(smax, s2);
+      } else {
+#pragma unroll
+        for (int me = 0; me < N; ++me) W.w1[me] = W.w2[me] = 0.0;
+      }
+#pragma unroll
+      for (int me = 0; me < N; ++me) {
+        S.sw1[me][sl] = W.w1[me];
+        S.sw2[me][sl] = W.w2[me];
+      }
+      S.ss2[sl] = s2;
+    }
+    __syncthreads();
+    if constexpr (SO) {  // phase C: correction flux at interface k = s - 1 + r into flux slot (r+1)TX + c
+      const int k = s - 1 + r;
+      const int w = (r + 1) * TX + cx;  // interface k; k-1 at w - TX, k+1 at w + TX
+      double ft[N];
+#pragma unroll
+      for (int me = 0; me < N; ++me) ft[me] = 0.0;
+      if (k <= my + 1) {
+        WavesN<N> Wm, W, Wp;
+#pragma unroll
+        for (int me = 0; me < N; ++me) {
+          Wm.w1[me] = S.sw1[me][w - TX], Wm.w2[me] = S.sw2[me][w - TX];
+          W.w1[me] = S.sw1[me][w], W.w2[me] = S.sw2[me][w];
+          Wp.w1[me] = S.sw1[me][w + TX], Wp.w2[me] = S.sw2[me][w + TX];
+        }
+        // cells k-1 and k sit in the slots of interfaces k-1 and k
+        corr_flux<N, LIM>(Wm, W, Wp, S.ss2[w], k <= my, dtod, S.sk[w - TX], S.sk[w], ft);
+      }
+#pragma unroll
+      for (int me = 0; me < N; ++me) S.sft[me][(r + 1) * TX + cx] = ft[me];
+      __syncthreads();
+    }
+    {  // phase D: update of cell j = s - 2 + r (cell and interface slot rTX + c)
+      const int j = s - 2 + r;
+      if (active && j >= j0 && j <= jlast) {
+        const int c = r * TX + cx;
+        const double dtk = dtod / S.sk[c];
+        const double sp = S.ss2[c];
+        const double sm = -S.ss2[c + TX];
+        const long long o = (long long)(j + 1) * P + (i + 1);
+#pragma unroll
+        for (int me = 0; me < N; ++me) {
+          const double ap = sp * S.sw2[me][c];
+          const double am = sm * S.sw1[me][c + TX];
+          double q = S.sq[me][c] - dtk * (gam * ap + gam * am);
+          if constexpr (SO) q = q - dtk * (S.sft[me][c + TX] - S.sft[me][c]);
+          outp[o + me * g.plane] = q;
+        }
+        if (i == 1 || i == mx) {  // the pre-step ghost columns beside the edge columns
+          const long long ob = (long long)(j + 1) * P;
+          const int g0 = i == 1 ? -1 : mx + 1;
+#pragma unroll
+          for (int gcol = g0; gcol <= g0 + 1; ++gcol)
+#pragma unroll
+            for (int me = 0; me < N; ++me) outp[ob + gcol + 1 + me * g.plane] = pre[ob + gcol + 1 + me * g.plane];
+        }
+      }
+    }
+    // History: rows L, L+1 -> 0, 1 (cells, interfaces) and flux row L -> 0.  Only threads of
+    // rows 0 and 1 read those rows in phase D, and they share warp 0 with the copying threads.
+    if (threadIdx.x < 32) __syncwarp();
+    if (r < 2) {
+      const int from = (L + r) * TX + cx, to = r * TX + cx;
+#pragma unroll
+      for (int me = 0; me < N; ++me) {
+        S.sq[me][to] = S.sq[me][from];
+        S.sf[me][to] = S.sf[me][from];
+        S.sw1[me][to] = S.sw1[me][from];
+        S.sw2[me][to] = S.sw2[me][from];
+      }
+      S.ss[to] = S.ss[from];
+      S.sk[to] = S.sk[from];
+      S.ss2[to] = S.ss2[from];
+      if (r == 0) {
+#pragma unroll
+        for (int me = 0; me < N; ++me) S.sft[me][cx] = S.sft[me][L * TX + cx];
+      }
+    }
+    __syncthreads();
+  }
+  if (active && r < 4) {  // the pre-step ghost rows of the band's columns
+    auto copy_cell = [&](int cj) {
+      const long long o = (long long)(cj + 1) * P + (i + 1);
+#pragma unroll
+      for (int me = 0; me < N; ++me) outp[o + me * g.plane] = pre[o + me * g.plane];
+    };
+    if (r < 2 && j0 == 1) copy_cell(-1 + r);
+    if (r >= 2 && jlast == my) copy_cell(my + r - 1);
+  }
+  smax_acc = fmax(smax_acc, smax);
+  bad_acc |= bad;
+}
+
+
 }  // namespace gen
 }  // namespace pcl

@@ -204,3 +204,28 @@ def test_n_equation_context_rules(pcl):
         Solver(_n_control(16, 16, 4), precision=ctl.PRECISION_MIXED)   # mixed: three equations
     with pytest.raises(_lib.PclError):
         Solver(_n_control(16, 16, 5))                                  # no module has five
+
+
+@pytest.mark.parametrize("module,n,prm", [(ctl.EQ_ADVECTION, 1, (1.0, -0.6)), (ctl.EQ_BURGERS, 1, ()),
+                                          (ctl.EQ_ACOUSTICS, 3, (2.0, 0.5)),
+                                          (ctl.EQ_SHALLOW_WATER_TRACER, 4, (ctl.GRAV_REFERENCE,))])
+def test_generic_eta_shapes_agree(pcl, module, n, prm):
+    """The generic path's eta sweep in bands (the default) and in column windows
+    (pcl_set_sweep_shape) gives the same bits, on a grid whose sizes are multiples of neither the
+    band width nor the chunk height nor the window width."""
+    from paraclaws_b200 import _lib
+    outs = []
+    for shape in (_lib.PCL_SHAPE_BAND, _lib.PCL_SHAPE_WINDOW):
+        c = _n_control(133, 271, n, limiter=1, bc=1, time_final=0.05)
+        s = Solver(c)
+        s.set_equation(module, prm)
+        s.set_sweep_shape(shape)
+        assert s.sweep_shape() == shape
+        s.upload(_n_state(133, 271, n, module))
+        s.update_rank_boundaries()
+        st = s.advance()
+        assert st.status == 0 and st.accepted > 5
+        outs.append((s.download(), s.step_log().dt))
+        s.close()
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][0].view(np.int64), outs[1][0].view(np.int64))
