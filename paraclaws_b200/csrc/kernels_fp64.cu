@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g,
   double smax = 0.0;
   int bad = 0;
   const int j0 = 1 + blockIdx.y * chunk;
-  ysweep_band<kBT, kBX, LIM, SO, MK, kOptFastDiv, true>(g, -1 + blockIdx.x * kBX, j0, j0 + chunk - 1, S, smax,
+  ysweep_band<kBT, kBX, LIM, SO, MK, kOptFastDiv, true>(g, (int)blockIdx.x * kBX - 1, j0, j0 + chunk - 1, S, smax,
                                                         bad);
   block_max_to<kBT>(&g.ctl->smax_y, smax, S.red);
   if (bad) atomicOr(&g.ctl->status, bad);

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kGBT, 6) yband_gen_kernel(GridDev g, int chunk
   double smax = 0.0;
   int bad = 0;
   const int j0 = 1 + blockIdx.y * chunk;
-  gen::ysweep_band<kGBT, kGBX, N, LIM, SO>(g, -1 + blockIdx.x * kGBX, j0, j0 + chunk - 1, S, smax, bad);
+  gen::ysweep_band<kGBT, kGBX, N, LIM, SO>(g, (int)blockIdx.x * kGBX - 1, j0, j0 + chunk - 1, S, smax, bad);
   block_max_to<kGBT>(&g.ctl->smax_y, smax, S.red);
   if (bad) atomicOr(&g.ctl->status, bad);
 }
