@@ -278,7 +278,9 @@ int pcl_get_stats(pcl_ctx* ctx, pcl_run_stats* stats);
 int pcl_reset_time_control(pcl_ctx* ctx);
 /* Diagnostic: run `reps` device-loop attempts with a CUDA event around every kernel and return
    the mean duration of each kernel kind in avg_ms[] (FP64: xi sweep, eta sweep, time control,
-   ghost fill; mixed: fused sweep, time control, ghost fill); *nkinds = entries written. */
+   ghost fill; mixed: fused sweep, time control, ghost fill); *nkinds = entries written.  The
+   attempts advance the run: on a context that reaches its end time or accepted-step cap during
+   them, the remaining kernels return at once and the means come out too short. */
 int pcl_profile_kernels(pcl_ctx* ctx, int reps, double* avg_ms, int* nkinds);
 /* Copy up to cap records of the device step log; *n = records logged so far. */
 int pcl_get_step_log(pcl_ctx* ctx, pcl_step_record* out, long long cap, long long* n);
