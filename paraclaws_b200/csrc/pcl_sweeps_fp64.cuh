@@ -364,7 +364,7 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
 }
 
 // ------------------------------------------------------------------------------------------
-// eta sweep in bands (the shape for grids too small to fill the GPU with column windows).  A CTA
+// eta sweep in bands (the default shape at every grid size; the batch's eta items).  A CTA
 // walks down a band of TX columns over rows j0 .. j1 in steps of L = NT/TX rows, running the xi
 // sweep's four shared-memory phases along the columns: slot (r, c) = (row, column in the band),
 // so a warp's loads are TX*8 contiguous bytes on each of 32/TX rows.  The last two cells, the last
@@ -374,9 +374,9 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
 // outside 1 .. m_xi are computed on a clamped column and written nowhere.
 //
 // Semantics of ysweep_strip: rows 1 .. m_eta from the xi-swept buffer, the ghost rows from the
-// pre-step buffer (main.f90:210 runs before the ghost fill at :246); getJakobi's status over rows -1 .. m_eta+1; waves of interfaces beyond
-// m_eta+1 are zero and the interface m_eta+1 is unlimited; the pre-step ghost cells carried into
-// the new buffer.  The first step of a CTA starts at s = j0-2 with empty history: its interface
+// pre-step buffer (main.f90:210 runs before the ghost fill at :246); getJakobi's status over rows
+// -1 .. m_eta+1; waves of interfaces beyond m_eta+1 are zero and the interface m_eta+1 is
+// unlimited; the pre-step ghost cells carried into the new buffer.  The first step of a CTA starts at s = j0-2 with empty history: its interface
 // s and the correction fluxes and updates that would read the history are never used (updates
 // start at row j0).  The caller checks the xi-sweep validity (eta_valid) and reduces smax and
 // the status bits over the CTA.
