@@ -1,9 +1,10 @@
 """The FP64 eta sweep's two shapes (include/paraclaws_b200.h: pcl_set_sweep_shape) against the
-oracle: column windows and 4-column bands each reproduce the oracle's state, dt sequence, CFL
+oracle: column windows and 16-column bands each reproduce the oracle's state, dt sequence, CFL
 and accept/reject flags bit for bit, on grids whose sizes are not multiples of the band width,
 chunk height or window width, for every limiter, the unlimited correction, first order, the three
 boundary codes and a domain whose capacities are not exactly 1.  The automatic choice follows
-the grid size and changes nothing either."""
+the equation module and g (windows only where the shared-reciprocal quotient is out of range)
+and changes nothing either."""
 import dataclasses
 
 import numpy as np
@@ -69,8 +70,9 @@ def test_shape_matches_oracle(pcl, oracle_lib, shape, name, grid, over, tf):
 
 
 def test_shapes_agree_on_a_large_grid(pcl):
-    """1536 x 2100 (the automatic choice is a band here, windows above a few thousand cells a
-    side): both forced shapes give the same bits over 12 attempted steps."""
+    """1536 x 2100: 97 bands of 33 chunks of 64 rows each on a 148-SM part (the chunk seams and
+    the history rows carried across them are exercised): both forced shapes give the same bits
+    over 12 accepted steps."""
     c = dataclasses.replace(ctl.dam_break_control(1536, limiter=1, bc=1, time_final=1e9), m_eta=2100)
     q = ic.gaussian_bumps(1536, 2100, seed=3)
     cu = ctl.CustomSettings(max_accepted_steps=12)
