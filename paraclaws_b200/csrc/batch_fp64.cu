@@ -45,7 +45,7 @@ __device__ __forceinline__ void run_item(const GridDev& g, int kind, int a, int 
     xsweep_finish<kThreads>(g, smax, bad, S.x);
   } else {
     if (!eta_valid(g)) return;  // the same answer for every thread: all xi items are done
-    ysweep_band<kThreads, kBandCols, LIM, SO, MK, OPT>(g, a, b, b + v.y_rows - 1, S.y, smax, bad);
+    ysweep_band<kThreads, kBandCols, LIM, SO, MK, OPT, false, false>(g, a, b, b + v.y_rows - 1, S.y, smax, bad);
     block_max_to<kThreads>(&g.ctl->smax_y, smax, S.y.red);
     if (bad) atomicOr(&g.ctl->status, bad);
   }

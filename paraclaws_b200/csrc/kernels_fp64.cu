@@ -24,9 +24,11 @@ namespace {
 // 256-thread CTAs with 252-cell segments, 4 per SM: 0.415).
 // The eta sweep has two shapes.  Column windows (ysweep_strip) at 6 CTAs of 128 threads per SM
 // (80 registers, a few spilled window values) with 24-row strips (16 rows: +1%, 32: +1%).  Bands
-// (ysweep_band), 64 registers, no spills, each thread staging its cell of the next step by
+// (ysweep_band), 64 registers (4 bytes spilled), each thread staging its cell of the next step by
 // cp.async while the phases of this one run: 16 columns x 16 rows per step in 256-thread CTAs,
-// 4 per SM (55 KB of shared memory each), a barrier per 256 cells.  Against 8 columns x 16 rows
+// 4 per SM (50 KB of shared memory each), three barriers per 256 cells (cell states by step
+// parity: 0.452 ms at 4096^2 against 0.459 ms with a fourth barrier closing each step and the
+// staging in a separate buffer, same box, back to back).  Against 8 columns x 16 rows
 // in 128-thread CTAs, 8 per SM: eta sweep 0.460 against 0.465 ms at 4096^2, whole step 3.13
 // against 3.15 ms at 8192^2; 8 columns x 32 rows in 256 threads: 0.503 ms; 16 columns x 32 rows
 // in 512 threads (2 CTAs per SM): 0.521 ms.  Lab, eta sweep in ms on bumps after 8 / 200 steps,
@@ -77,7 +79,7 @@ __global__ void __launch_bounds__(NTX, kYMinBlocks) ysweep_fp64_kernel(GridDev g
 template <int LIM, bool SO, int MK>
 __global__ void __launch_bounds__(kBT, kBMinBlocks) yband_fp64_kernel(GridDev g, int chunk) {
   extern __shared__ __align__(16) unsigned char band_smem[];
-  auto& S = *reinterpret_cast<YBSmem<kBT, kBX, true, MK == kMetricMapped>*>(band_smem);
+  auto& S = *reinterpret_cast<YBSmem<kBT, kBX, MK == kMetricMapped>*>(band_smem);
   if (g.ctl->done || !eta_valid(g)) return;
   double smax = 0.0;
   int bad = 0;
@@ -128,8 +130,8 @@ void launch_y_t(const GridDev& g, cudaStream_t st) {
     int chunk = 256;
     while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
     dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
-    // 55 KB of dynamic shared memory: allowed once per device for each build of the kernel
-    constexpr int smem = (int)sizeof(YBSmem<kBT, kBX, true, MK == kMetricMapped>);
+    // 50 KB (mapped grids: 54 KB) of dynamic shared memory: allowed once per device for each build
+    constexpr int smem = (int)sizeof(YBSmem<kBT, kBX, MK == kMetricMapped>);
     static std::atomic<unsigned long long> allowed{0};
     int dev = 0;
     cudaGetDevice(&dev);

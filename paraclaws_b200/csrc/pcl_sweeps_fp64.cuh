@@ -373,6 +373,17 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
 // i = -1 + TX*k (a 32-byte sector boundary, the pitch being a multiple of 32 doubles); columns
 // outside 1 .. m_xi are computed on a clamped column and written nowhere.
 //
+// PB (parity buffers): three CTA barriers per step (after phases A, B and C).  The cell states,
+// capacities and face ratios, which phase D reads while faster threads already fill the next
+// step's phase A, are kept per step parity; the next step's cells are staged (PF: cp.async,
+// right after the barrier that ends this step's phase A) or loaded into the other parity.
+// History rows move at two points: the phase-A arrays right after the phase-B barrier (nothing
+// of this step reads their rows 0, 1 after it; the next phase A writes rows 2 and up only), the
+// phase-B and C arrays after phase D in the warp that reads their rows 0, 1 (the next step
+// writes them only after its phase-A barrier).  Without PB (less shared memory: the batch's
+// items, whose kernel keeps a stack in L1) one copy of each array, every history row moved after
+// phase D, and a fourth barrier closes the step.
+//
 // Semantics of ysweep_strip: rows 1 .. m_eta from the xi-swept buffer, the ghost rows from the
 // pre-step buffer (main.f90:210 runs before the ghost fill at :246); getJakobi's status over rows
 // -1 .. m_eta+1; waves of interfaces beyond m_eta+1 are zero and the interface m_eta+1 is
@@ -381,40 +392,36 @@ __device__ __forceinline__ void ysweep_strip(const GridDev& g, int col0, int j0,
 // start at row j0).  The caller checks the xi-sweep validity (eta_valid) and reduces smax and
 // the status bits over the CTA.
 // ------------------------------------------------------------------------------------------
-template <int NT, bool PF>
-struct YBStage {
-  double stg[2][3][NT];  // the cells of the next step, staged by cp.async while this one runs
-};
-template <int NT>
-struct YBStage<NT, false> {};
-template <int SLOTS, bool MP>
+template <int SLOTS, int NP, bool MP>
 struct YBMapped {
-  double slr[SLOTS];  // mapped grids: length ratio of the eta face below the cell
+  double slr[NP][SLOTS];  // mapped grids: length ratio of the eta face below the cell
 };
-template <int SLOTS>
-struct YBMapped<SLOTS, false> {};
+template <int SLOTS, int NP>
+struct YBMapped<SLOTS, NP, false> {};
 
-// PF: staging of the next step's cells; MP: mapped-grid metrics (the batch and uniform grids
-// leave both out when they do not use them, for shared memory).
-template <int NT, int TX, bool PF = false, bool MP = true>
-struct YBSmem : YBStage<NT, PF>, YBMapped<(NT / TX + 2) * TX, MP> {
-  static constexpr int L = NT / TX;
-  double sq[3][(L + 2) * TX], sf[3][(L + 2) * TX], ss[(L + 2) * TX], sk[(L + 2) * TX];
-  double sw1[3][(L + 2) * TX], sw2[3][(L + 2) * TX], ss2[(L + 2) * TX];
+// MP: mapped-grid metrics (the batch and uniform grids leave them out, for shared memory);
+// PB: parity buffers.
+template <int NT, int TX, bool MP = true, bool PB = true>
+struct YBSmem : YBMapped<(NT / TX + 2) * TX, PB ? 2 : 1, MP> {
+  static constexpr int L = NT / TX, SL = (L + 2) * TX, NP = PB ? 2 : 1;
+  double sq[NP][3][SL], sk[NP][SL];  // cell states and capacities (by step parity with PB)
+  double sf[3][SL], ss[SL];
+  double sw1[3][SL], sw2[3][SL], ss2[SL];
   double sft[3][(L + 1) * TX];
   double red[NT / 32];
-  bool sok[(L + 2) * TX];
+  bool sok[SL];
 };
 
-// PF: each thread stages its cell of the next step into shared memory (cp.async) before the
-// phases of this step, so the global loads overlap the four phases instead of opening them.
-template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0, bool PF = false>
+// PF: each thread stages its cell of the next step into shared memory (cp.async) while this
+// step's phases B .. D run, so the global loads do not open the step.
+template <int NT, int TX, int LIM, bool SO, int MK = kMetricTable, int OPT = 0, bool PF = false, bool PB = true>
 __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, int j1,
-                                            YBSmem<NT, TX, PF, MK == kMetricMapped>& S, double& smax_acc,
+                                            YBSmem<NT, TX, MK == kMetricMapped, PB>& S, double& smax_acc,
                                             int& bad_acc) {
   constexpr bool UM = MK == kMetricUnit, MP = MK == kMetricMapped;
   constexpr int L = NT / TX;
   static_assert(NT % 32 == 0 && TX <= 16 && L >= 4, "band shape: rows 0, 1 within warp 0");
+  static_assert(PB || !PF, "staging fills the other parity");
   const Ctl* ctl = g.ctl;
   const int cur = ctl->cur;
   const int xb = cur == 2 ? 0 : cur + 1;
@@ -434,68 +441,64 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
   double smax = 0.0;
   int bad = 0;
   const int jlast = min(j1, my);
-  // cell j = s + r of this thread's column into staging buffer b (rows past m_eta+2: nothing)
-  auto stage = [&](int s_, int b_) {
+  const int sa = (r + 2) * TX + cx;  // this thread's phase-A and phase-B slot
+  // cell j = s + r of this thread's column into its slot of parity p (rows past m_eta+2: nothing)
+  auto stage = [&](int s_, int p_) {
     if constexpr (PF) {
       const int j = s_ + r;
       if (j <= my + 2) {
         const double* src = (j >= 1 && j <= my) ? xsw : pre;
         const long long o = (long long)(j + 1) * P + (ic + 1);
-        cp_async8(&S.stg[b_][0][t], src + o);
-        cp_async8(&S.stg[b_][1][t], src + o + g.plane);
-        cp_async8(&S.stg[b_][2][t], src + o + 2 * g.plane);
+        cp_async8(&S.sq[p_][0][sa], src + o);
+        cp_async8(&S.sq[p_][1][sa], src + o + g.plane);
+        cp_async8(&S.sq[p_][2][sa], src + o + 2 * g.plane);
       }
       cp_async_commit();
     }
   };
   if constexpr (PF) stage(j0 - 2, 0);
 
-  int sb = 0;  // PF: staging buffer of this step
-  for (int s = j0 - 2; s - 2 <= jlast; s += L, sb ^= 1) {
-    if constexpr (PF) {
-      if (s + L - 2 <= jlast) {  // there is a next step: stage it, then wait for this one only
-        stage(s + L, sb ^ 1);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-    }
+  int p = 0;  // step parity (0 throughout without PB)
+  for (int s = j0 - 2; s - 2 <= jlast; s += L, p = PB ? p ^ 1 : 0) {
+    if constexpr (PF) cp_async_wait<0>();
     {  // phase A: cell j = s + r into slot (r+2)TX + c
       const int j = s + r;
-      const int sl = (r + 2) * TX + cx;
       if (j <= my + 2) {
-        const double* src = (j >= 1 && j <= my) ? xsw : pre;
         const long long o = (long long)(j + 1) * P + (ic + 1);
         double h, hu, hv;
         if constexpr (PF) {
-          h = S.stg[sb][0][t], hu = S.stg[sb][1][t], hv = S.stg[sb][2][t];
+          h = S.sq[p][0][sa], hu = S.sq[p][1][sa], hv = S.sq[p][2][sa];
         } else {
+          const double* src = (j >= 1 && j <= my) ? xsw : pre;
           h = src[o], hu = src[o + g.plane], hv = src[o + 2 * g.plane];
+          S.sq[p][0][sa] = h; S.sq[p][1][sa] = hu; S.sq[p][2][sa] = hv;
         }
         int cb = 0;
         const CellFlux F = cell_flux<1, OPT>(h, hu, hv, g.grav, &cb);
         if (j <= my + 1 && active) bad |= cb;
-        S.sq[0][sl] = h; S.sq[1][sl] = hu; S.sq[2][sl] = hv;
-        S.sf[0][sl] = F.f0; S.sf[1][sl] = F.f1; S.sf[2][sl] = F.f2;
-        S.ss[sl] = F.s;
-        if constexpr ((OPT & kOptFastDiv) != 0) S.sok[sl] = F.ok;
+        S.sf[0][sa] = F.f0; S.sf[1][sa] = F.f1; S.sf[2][sa] = F.f2;
+        S.ss[sa] = F.s;
+        if constexpr ((OPT & kOptFastDiv) != 0) S.sok[sa] = F.ok;
         if constexpr (MP) {
-          S.sk[sl] = __ldg(g.kap + o);
-          S.slr[sl] = __ldg(g.lry + o);
+          S.sk[p][sa] = __ldg(g.kap + o);
+          S.slr[p][sa] = __ldg(g.lry + o);
         } else if constexpr (!UM) {
-          S.sk[sl] = capacity(g.rowm, g.colm, ic, j, g.area_scale);
+          S.sk[p][sa] = capacity(g.rowm, g.colm, ic, j, g.area_scale);
         }
       }
     }
     __syncthreads();
+    if constexpr (PF) {  // the next step's cells into the other parity, read last by the previous phase D
+      if (s + L - 2 <= jlast) stage(s + L, p ^ 1);
+    }
     {  // phase B: interface k = s + r (cells k-1, k) into slot (r+2)TX + c
       const int k = s + r;
-      const int sl = (r + 2) * TX + cx, sm = sl - TX;
+      const int sl = sa, sm = sl - TX;
       Waves W;
       double s2 = 0.0;
       if (k <= my + 1 && k >= j0 - 1) {
-        const double qL[3] = {S.sq[0][sm], S.sq[1][sm], S.sq[2][sm]};
-        const double qR[3] = {S.sq[0][sl], S.sq[1][sl], S.sq[2][sl]};
+        const double qL[3] = {S.sq[p][0][sm], S.sq[p][1][sm], S.sq[p][2][sm]};
+        const double qR[3] = {S.sq[p][0][sl], S.sq[p][1][sl], S.sq[p][2][sl]};
         CellFlux FL = {S.sf[0][sm], S.sf[1][sm], S.sf[2][sm], S.ss[sm]};
         CellFlux FR = {S.sf[0][sl], S.sf[1][sl], S.sf[2][sl], S.ss[sl]};
         if constexpr ((OPT & kOptFastDiv) != 0) FL.ok = S.sok[sm], FR.ok = S.sok[sl];
@@ -513,13 +516,29 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
       S.ss2[sl] = s2;
     }
     __syncthreads();
+    // history of the phase-A arrays: rows L, L+1 -> 0, 1 (states and metrics: of parity p ^ 1)
+    auto history_a = [&](int pn) {
+      if (r < 2) {
+        const int from = (L + r) * TX + cx, to = r * TX + cx;
+#pragma unroll
+        for (int me = 0; me < 3; ++me) {
+          S.sq[pn][me][to] = S.sq[p][me][from];
+          S.sf[me][to] = S.sf[me][from];
+        }
+        S.ss[to] = S.ss[from];
+        if constexpr ((OPT & kOptFastDiv) != 0) S.sok[to] = S.sok[from];
+        if constexpr (MP) S.slr[pn][to] = S.slr[p][from];
+        if constexpr (MP || !UM) S.sk[pn][to] = S.sk[p][from];
+      }
+    };
+    if constexpr (PB) history_a(p ^ 1);
     if constexpr (SO) {  // phase C: correction flux at interface k = s - 1 + r into ft slot (r+1)TX + c
       const int k = s - 1 + r;
       const int w = (r + 1) * TX + cx;  // interface k's slot; k-1 at w - TX, k+1 at w + TX
       double ft[3] = {0.0, 0.0, 0.0};
       if (k <= my + 1) {
         const double s2 = S.ss2[w];
-        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, S.sk[w - TX], S.sk[w]);
+        const double cf = UM ? corr_coef_unit(s2, dtod) : corr_coef(s2, dtod, S.sk[p][w - TX], S.sk[p][w]);
         if (cf != 0.0) {
           const double w1[3] = {S.sw1[0][w], S.sw1[1][w], S.sw1[2][w]};
           const double w2[3] = {S.sw2[0][w], S.sw2[1][w], S.sw2[2][w]};
@@ -551,8 +570,8 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
       if (active && j >= j0 && j <= jlast) {
         const int c = r * TX + cx;
         double gl = gam, gr = gam;  // faces below and above the cell
-        if constexpr (MP) gl = S.slr[c], gr = S.slr[c + TX];
-        const double dtk = UM ? dtod : dtod / S.sk[c];
+        if constexpr (MP) gl = S.slr[p][c], gr = S.slr[p][c + TX];
+        const double dtk = UM ? dtod : dtod / S.sk[p][c];
         const double sp = S.ss2[c];
         const double sm = -S.ss2[c + TX];
         const long long o = (long long)(j + 1) * P + (i + 1);
@@ -560,7 +579,7 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
         for (int me = 0; me < 3; ++me) {
           const double ap = sp * S.sw2[me][c];
           const double am = sm * S.sw1[me][c + TX];
-          double q = UM ? S.sq[me][c] - dtk * (ap + am) : S.sq[me][c] - dtk * (gl * ap + gr * am);
+          double q = UM ? S.sq[p][me][c] - dtk * (ap + am) : S.sq[p][me][c] - dtk * (gl * ap + gr * am);
           if constexpr (SO) q = q - dtk * (S.sft[me][c + TX] - S.sft[me][c]);
           outp[o + me * g.plane] = q;
         }
@@ -574,32 +593,30 @@ __device__ __forceinline__ void ysweep_band(const GridDev& g, int i0, int j0, in
         }
       }
     }
-    // History: cells and interfaces of rows L, L+1 -> 0, 1, correction flux L -> 0.  Phase D
-    // reads rows 0 and 1 of those arrays only in threads r = 0, 1 (row 2 and up belong to
-    // later rows), which share warp 0 with the copying threads (32/TX >= 2 rows per warp): a
-    // warp barrier orders them.  The rows copied from were final before phase D.
+    // History of the interfaces (rows L, L+1 -> 0, 1) and the correction flux (L -> 0), and
+    // without PB of the phase-A arrays too.  Phase D reads rows 0 and 1 of those arrays only in
+    // threads r = 0, 1 (row 2 and up belong to later rows), which share warp 0 with the copying
+    // threads (32/TX >= 2 rows per warp): a warp barrier orders them.  The rows copied from were
+    // final before phase D.  With PB the next step writes these arrays only after its phase-A
+    // barrier, which this warp reaches after the copy: no closing CTA barrier.
     if (threadIdx.x < 32) __syncwarp();
+    if constexpr (!PB) history_a(0);
     if (r < 2) {
       const int from = (L + r) * TX + cx, to = r * TX + cx;
 #pragma unroll
       for (int me = 0; me < 3; ++me) {
-        S.sq[me][to] = S.sq[me][from];
-        S.sf[me][to] = S.sf[me][from];
         S.sw1[me][to] = S.sw1[me][from];
         S.sw2[me][to] = S.sw2[me][from];
       }
-      S.ss[to] = S.ss[from];
       S.ss2[to] = S.ss2[from];
-      if constexpr ((OPT & kOptFastDiv) != 0) S.sok[to] = S.sok[from];
-      if constexpr (MP) S.slr[to] = S.slr[from];
-      if constexpr (MP || !UM) S.sk[to] = S.sk[from];
       if (r == 0) {
 #pragma unroll
         for (int me = 0; me < 3; ++me) S.sft[me][cx] = S.sft[me][L * TX + cx];
       }
     }
-    __syncthreads();
+    if constexpr (!PB) __syncthreads();
   }
+  if constexpr (PB) __syncthreads();  // the last step's phase D has read S before the caller reuses it
   if (active && r < 4) {  // the pre-step ghost rows of the band's columns
     auto copy_cell = [&](int ci, int cj) {
       const long long o = (long long)(cj + 1) * P + (ci + 1);
