@@ -25,18 +25,22 @@ namespace {
 // The eta sweep has two shapes.  Column windows (ysweep_strip) at 6 CTAs of 128 threads per SM
 // (80 registers, a few spilled window values) with 24-row strips (16 rows: +1%, 32: +1%).  Bands
 // (ysweep_band), 64 registers (4 bytes spilled), each thread staging its cell of the next step by
-// cp.async while the phases of this one run: 16 columns x 16 rows per step in 256-thread CTAs,
-// 4 per SM (50 KB of shared memory each), three barriers per 256 cells (cell states by step
-// parity: 0.452 ms at 4096^2 against 0.459 ms with a fourth barrier closing each step and the
-// staging in a separate buffer, same box, back to back).  Against 8 columns x 16 rows
-// in 128-thread CTAs, 8 per SM: eta sweep 0.460 against 0.465 ms at 4096^2, whole step 3.13
-// against 3.15 ms at 8192^2; 8 columns x 32 rows in 256 threads: 0.503 ms; 16 columns x 32 rows
-// in 512 threads (2 CTAs per SM): 0.521 ms.  Lab, eta sweep in ms on bumps after 8 / 200 steps,
-// windows against 8-column bands: 4096^2 0.482 / 0.499 against 0.465 / 0.468 (256-row chunks);
-// 2048^2 0.155 / 0.156 against 0.141 / 0.144 (128-row chunks).  Without the staging the bands
-// take 0.473 / 0.480 at 4096^2; 4-column bands 0.548 / 0.556 (their rows are single 32-byte
-// sectors).  Bands run wherever the shared-reciprocal quotients do; the chunk is the tallest of
-// 256, 128 and 64 rows that still makes kYWaves waves of CTAs.  Measured and dropped: the two
+// cp.async while the phases of this one run, cell states by step parity (three barriers per
+// step): 16 columns x 8 rows per step in 128-thread CTAs, 8 per SM (28 KB of shared memory
+// each).  Same box, back to back, eta sweep in ms: 2048^2 0.134 (64-row chunks) against 0.142
+// for 16 columns x 16 rows in 256-thread CTAs at 4 per SM (128-row chunks); 4096^2 0.433
+// (128-row chunks) against 0.453 (256); 8192^2 1.544 against 1.623 (256 both); 8 columns x 16
+// rows in 128-thread CTAs: 0.141, 0.458, 1.645.  The 256-thread CTAs had gained from the
+// parity copies themselves: 0.452 against 0.459 ms at 4096^2 with a fourth barrier closing each
+// step and the staging in a separate buffer.  Before them: 8 columns x 32 rows in 256 threads
+// 0.503 ms, 16 columns x 32 rows in 512 threads (2 CTAs per SM) 0.521 ms.  Lab, eta sweep in
+// ms on bumps after 8 / 200 steps, windows against 8-column bands: 4096^2 0.482 / 0.499
+// against 0.465 / 0.468; 2048^2 0.155 / 0.156 against 0.141 / 0.144.  Without the staging the
+// bands took 0.473 / 0.480 at 4096^2; 4-column bands 0.548 / 0.556 (their rows are single
+// 32-byte sectors).  Bands run wherever the shared-reciprocal quotients do; the chunk is the
+// tallest of 256, 128 and 64 rows that still makes kYWaves waves of CTAs.  Six waves of 8
+// CTAs per SM picked the fastest chunk, measured, at 1024^2 and 2048^2 (64), 4096^2 (128: 256
+// leaves 3.5 waves, the last one half empty) and 8192^2 (256).  Measured and dropped: the two
 // shortcuts and an unrolled row loop in the windows (more registers, more spills); tiles that
 // recompute their 4 halo rows instead of carrying them (0.489 ms at 4096^2 at best); an xi sweep
 // that stores its result transposed so the eta sweep can read contiguous lines (0.645 + 0.653
@@ -48,10 +52,10 @@ constexpr int kXRows = 8;  // rows of one segment per xi-sweep CTA
 constexpr int kYT = 128;   // columns of an eta-sweep window CTA
 constexpr int kYMinBlocks = 6;
 constexpr int kYS = 24;    // rows of an eta-sweep strip
-constexpr int kBT = 256;   // threads of an eta-sweep band CTA
+constexpr int kBT = 128;   // threads of an eta-sweep band CTA
 constexpr int kBX = 16;    // columns of a band
-constexpr int kBMinBlocks = 4;
-constexpr int kYWaves = 3;
+constexpr int kBMinBlocks = 8;
+constexpr int kYWaves = 6;
 
 // A CTA sweeps R consecutive rows of one segment (blockIdx.y*R ..), strided by gridDim.y*R
 // when the grid has more rows than one launch's blocks cover.
@@ -130,7 +134,7 @@ void launch_y_t(const GridDev& g, cudaStream_t st) {
     int chunk = 256;
     while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
     dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
-    // 50 KB (mapped grids: 54 KB) of dynamic shared memory: allowed once per device for each build
+    // 28 KB (mapped grids: 30 KB) of dynamic shared memory: allowed once per device for each build
     constexpr int smem = (int)sizeof(YBSmem<kBT, kBX, MK == kMetricMapped>);
     static std::atomic<unsigned long long> allowed{0};
     int dev = 0;
