@@ -38,9 +38,11 @@ namespace {
 // against 0.465 / 0.468; 2048^2 0.155 / 0.156 against 0.141 / 0.144.  Without the staging the
 // bands took 0.473 / 0.480 at 4096^2; 4-column bands 0.548 / 0.556 (their rows are single
 // 32-byte sectors).  Bands run wherever the shared-reciprocal quotients do; the chunk is the
-// tallest of 256, 128 and 64 rows that still makes kYWaves waves of CTAs.  Six waves of 8
-// CTAs per SM picked the fastest chunk, measured, at 1024^2 and 2048^2 (64), 4096^2 (128: 256
-// leaves 3.5 waves, the last one half empty) and 8192^2 (256).  Measured and dropped: the two
+// tallest of 256, 128 and 64 rows that still makes kYWaves waves of CTAs, less the 4-row halo.
+// Six waves of 8 CTAs per SM picked the fastest chunk, measured, at 1024^2 and 2048^2 (64),
+// 4096^2 (128: 256 leaves 3.5 waves, the last one half empty) and 8192^2 (256); the halo
+// rows off (252, 124, 60: no step half used) took the eta sweep from 0.046 / 0.134 / 0.431 /
+// 1.543 ms to 0.045 / 0.127 / 0.420 / 1.513 ms at those sizes.  Measured and dropped: the two
 // shortcuts and an unrolled row loop in the windows (more registers, more spills); tiles that
 // recompute their 4 halo rows instead of carrying them (0.489 ms at 4096^2 at best); an xi sweep
 // that stores its result transposed so the eta sweep can read contiguous lines (0.645 + 0.653
@@ -131,8 +133,12 @@ void launch_y_t(const GridDev& g, cudaStream_t st) {
   dim3 gy((g.mx + kYT - 1) / kYT, (g.my + kYS - 1) / kYS);
   if (eta_shape_of(g) == kEtaBand) {
     const long long bands = (g.mx + 2 + kBX - 1) / kBX, want = (long long)kYWaves * kBMinBlocks * sm_count();
-    int chunk = 256;
-    while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
+    // A chunk of c rows takes (c + 4) / L steps of L = kBT / kBX rows (its first step fills the
+    // 4-row halo), so chunks 4 rows short of 256, 128 or 64 leave no step half used.
+    int c = 256;
+    while (c > 64 && bands * ((g.my + c - 5) / (c - 4)) < want) c /= 2;
+    const int chunk = c - 4;
+    static_assert((64 % (kBT / kBX)) == 0, "chunk heights: multiples of the step height, less the halo");
     dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
     // 28 KB (mapped grids: 30 KB) of dynamic shared memory: allowed once per device for each build
     constexpr int smem = (int)sizeof(YBSmem<kBT, kBX, MK == kMetricMapped>);
