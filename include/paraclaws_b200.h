@@ -313,9 +313,10 @@ int pcl_batch_stats(pcl_batch* batch, int slot, pcl_run_stats* stats);
 int pcl_batch_download(pcl_batch* batch, int slot, double* vars);
 int pcl_batch_get_step_log(pcl_batch* batch, int slot, pcl_step_record* out, long long cap, long long* n);
 /* Schedule of the persistent kernel (set by the autotuner): rows per mixed work item (0, the
-   default: chosen from the instances each time they change), rows per FP64 xi item, rows per FP64
-   eta item (a chunk of a 4-column band), CTAs per SM (0: the occupancy limit).  Results do not
-   depend on it. */
+   default: chosen from the instances each time they change), rows per FP64 xi item (default 8),
+   rows per FP64 eta item (a chunk of a 4-column band, default 124: 32 rows per step, the first
+   step filling a 4-row halo), CTAs per SM (0: the occupancy limit).  Results do not depend on
+   it. */
 int pcl_batch_set_schedule(pcl_batch* batch, int tile_rows, int x_rows, int y_rows, int blocks_per_sm);
 int pcl_batch_info(pcl_batch* batch, int* n_used, int* n_done, long long* cells, long long* device_bytes);
 void* pcl_batch_get_stream(pcl_batch* batch);

@@ -28,7 +28,7 @@ from .solver import Stats, StepLog, to_c_control
 class Schedule:
     tile_rows: int = 0      # rows per mixed work item (0: chosen from the instances as they change)
     x_rows: int = 8         # rows per FP64 xi item
-    y_rows: int = 128       # rows per FP64 eta item (a chunk of a 4-column band)
+    y_rows: int = 124       # rows per FP64 eta item (a chunk of a 4-column band; 32 rows per step, 4 of halo)
     blocks_per_sm: int = 0  # persistent CTAs per SM (0: occupancy limit)
 
 
@@ -136,7 +136,7 @@ class Batch:
 def candidate_schedules(precision: int) -> List[Schedule]:
     if precision == PRECISION_MIXED:
         return [Schedule(tile_rows=tr, blocks_per_sm=b) for tr in (0, 32, 64, 128, 256) for b in (0, 3)]
-    return [Schedule(x_rows=xr, y_rows=yr, blocks_per_sm=b) for xr in (8, 16) for yr in (64, 128, 256, 512)
+    return [Schedule(x_rows=xr, y_rows=yr, blocks_per_sm=b) for xr in (8, 16) for yr in (60, 124, 252, 508)
             for b in (0, 6)]
 
 

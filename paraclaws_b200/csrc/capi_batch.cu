@@ -78,7 +78,9 @@ struct pcl_batch {
   bool dirty = true;
   int n_items = 0;
   // schedule (the autotuner's knobs)
-  int x_rows = 8, y_rows = 128, tile_rows = 0, blocks_per_sm = 0;  // tile_rows 0: chosen per membership
+  // tile_rows 0: chosen per membership.  y_rows: an eta item of c rows takes (c + 4) / 32 steps
+  // of its band (the first fills the 4-row halo), so 124 leaves no step half used.
+  int x_rows = 8, y_rows = 124, tile_rows = 0, blocks_per_sm = 0;
   int tile_rows_eff = 64;  // rows per mixed item in the current items (a launch parameter)
   int desc_base = -1;  // mixed: first descriptor of this batch in the constant pool (-1: none)
   int mode = -1;       // mixed: the mode every instance shares (the specialised build), or -1
