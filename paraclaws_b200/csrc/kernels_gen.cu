@@ -14,9 +14,10 @@ constexpr int kGXRows = 4; // rows of one segment per xi-sweep CTA
 constexpr int kGYT = 128;  // columns of an eta-sweep window CTA
 constexpr int kGYS = 32;   // rows of an eta-sweep strip
 // Eta sweep in bands (the default; gen::ysweep_band): 128-thread CTAs on 8-column bands, 16 rows
-// per step, chunks of 256 rows halved to 128 or 64 while the grid makes fewer than 3 waves, 6 CTAs
-// per SM.  At 4096^2 the dam-break module runs at 10.7 G cell-updates/s against 9.1 G with the
-// column windows (5 CTAs per SM without the register cap: 10.4 G), acoustics 12.8 G either way.
+// per step, chunks of 252 rows, 124 or 60 while the grid makes fewer than 3 waves, 6 CTAs per SM.
+// At 4096^2 the dam-break module runs at 11.0 G cell-updates/s (10.7 G with 256-row chunks, whose
+// last step ran half used) against 9.1 G with the column windows (5 CTAs per SM without the
+// register cap: 10.4 G); acoustics 13.1 G (12.8 G with 256-row chunks and with the windows).
 constexpr int kGBT = 128;
 constexpr int kGBX = 8;
 
@@ -81,8 +82,11 @@ struct GenLaunch {
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, yband_gen_kernel<N, LIM, SO>, kGBT, 0);
     const long long bands = (g.mx + 2 + kGBX - 1) / kGBX, want = 3LL * (occ > 0 ? occ : 1) * sm_count_gen();
-    int chunk = 256;
-    while (chunk > 64 && bands * ((g.my + chunk - 1) / chunk) < want) chunk /= 2;
+    // a chunk of c rows takes (c + 4) / 16 steps (the first fills the 4-row halo): chunks 4 rows
+    // short of 256, 128 or 64 leave no step half used
+    int c = 256;
+    while (c > 64 && bands * ((g.my + c - 5) / (c - 4)) < want) c /= 2;
+    const int chunk = c - 4;
     dim3 gb((unsigned)bands, (g.my + chunk - 1) / chunk);
     yband_gen_kernel<N, LIM, SO><<<gb, kGBT, 0, st>>>(g, chunk);
   }
