@@ -70,7 +70,7 @@ def test_shape_matches_oracle(pcl, oracle_lib, shape, name, grid, over, tf):
 
 
 def test_shapes_agree_on_a_large_grid(pcl):
-    """1536 x 2100: 97 bands of 33 chunks of 64 rows each on a 148-SM part (the chunk seams and
+    """1536 x 2100: 97 bands of 35 chunks of 60 rows each on a 148-SM part (the chunk seams and
     the history rows carried across them are exercised): both forced shapes give the same bits
     over 12 accepted steps."""
     c = dataclasses.replace(ctl.dam_break_control(1536, limiter=1, bc=1, time_final=1e9), m_eta=2100)
